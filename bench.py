@@ -1,0 +1,557 @@
+#!/usr/bin/env python
+"""Headline benchmark: pull-direction Jacobi PageRank (PageRankPull) on the
+Kronecker scale-25 graph (edge factor 16, RMAT 0.57/0.19/0.19, symmetrized,
+2^25 vertices, ~1.05e9 directed edges), float scores, damping 0.85,
+epsilon 1e-4, at most 20 sweeps -- the configuration the reference's
+pr_spmv -g 25 runs.
+
+One step = one complete solve (init, sweeps until the L1 change < epsilon,
+scores written in the caller's vertex order).  Prints ONE JSON line on rank 0:
+  value        GTEPS (directed edges x sweeps / second), whole job, inputs
+               resident in HBM, CUDA events on the launching stream
+  e2e          the same metric through the C-ABI host call (pr_gpu_run):
+               scores copied back to a pinned host buffer every step
+  roofline     the fused sweep kernel: algorithmic bytes per sweep
+               (4M + 20N + 4) / average sweep time vs measured HBM copy peak
+  cpu_baseline the reference's own PageRankPull (compiled from its sources)
+               on this host's cores, bounded sample
+  ppr          batched personalized PageRank (64 teleport vectors, Kronecker
+               scale 22) vs 64 sequential single-vector solves
+
+--gpus N under torchrun: N independent replicas (the path does not shard),
+timed as the max over ranks.  --impl reference: the reference arm (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+METRIC = "PR GTEPS & HBM GB/s vs peak; batched PPR vs plain GPU at L1<=1e-4"
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--graph", default="-g 25", help="pr_spmv graph options of the workload")
+    p.add_argument("--max-iters", type=int, default=20)
+    p.add_argument("--epsilon", type=float, default=1e-4)
+    p.add_argument("--ppr-graph", default="-g 22")
+    p.add_argument("--ppr-cols", type=int, default=64)
+    p.add_argument("--no-ppr", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-trials", type=int, default=2)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only: one barrier and one max per timing)
+
+class Dist:
+    def __init__(self, init: bool = True):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1 and init:
+            import datetime
+            import torch.distributed as dist
+            backend = "nccl" if _cuda_ok() else "gloo"
+            if backend == "nccl":
+                import torch
+                torch.cuda.set_device(self.local_rank)
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=900))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        dev = f"cuda:{self.local_rank}" if _cuda_ok() else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        dev = f"cuda:{self.local_rank}" if _cuda_ok() else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+def _cuda_ok() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.rows = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=5)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        if d.get("hbm_gbs"):
+            return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+def profiled_traffic(graph_args: str):
+    """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "pull_sweep_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        d = json.load(fh)
+    e = d.get(graph_args.strip())
+    return None if e is None else float(e["dram_bytes_per_sweep"])
+
+
+def sweep_bytes(n: int, m: int, directed: bool) -> int:
+    """Algorithmic bytes of one plain sweep: neighbour ids 4M, offsets 4(N+1),
+    contrib read 4N, old score 4N, new score 4N, next contrib 4N (+4(N+1)
+    out-offsets for a directed graph)."""
+    b = 4 * m + 20 * n + 4
+    if directed:
+        b += 4 * (n + 1)
+    return b
+
+
+def shm_graph_path(args_str: str) -> str:
+    h = hashlib.sha1(args_str.encode()).hexdigest()[:12]
+    base = "/dev/shm" if os.path.isdir("/dev/shm") else tempfile.gettempdir()
+    return os.path.join(base, f"gapbs_bench_{h}.sg")
+
+
+def load_graph(args_str: str, dist: Dist):
+    from gapbs_b200.graph import make_graph
+    if dist.world == 1:
+        return make_graph(args_str)
+    path = shm_graph_path(args_str)
+    if dist.rank == 0:
+        g = make_graph(args_str)
+        g.write_sg(path + ".tmp")
+        os.replace(path + ".tmp", path)
+    dist.barrier()
+    if dist.rank != 0:
+        g = make_graph(f"-f {path}")
+    dist.barrier()
+    if dist.rank == 0:
+        os.remove(path)
+    return g
+
+
+def ppr_teleports(g, k: int, seed: int):
+    """k teleport vectors, seed sets of log-uniform size in [1, 4096] drawn
+    from the non-isolated vertices; uniform 1/|S| on each set."""
+    rng = np.random.default_rng(seed)
+    cand = np.nonzero(np.diff(g.out_offsets) > 0)[0]
+    T = np.zeros((g.num_nodes, k), np.float32)
+    sizes = []
+    for c in range(k):
+        size = int(round(np.exp(rng.uniform(0.0, np.log(4096.0)))))
+        size = max(1, min(size, cand.size))
+        seeds = rng.choice(cand, size=size, replace=False)
+        T[seeds, c] = np.float32(1.0 / size)
+        sizes.append(size)
+    return T, sizes
+
+
+# ---------------------------------------------------------------------------
+# our arm
+
+def run_ours(a, dist: Dist):
+    import torch
+    from gapbs_b200 import PageRankEngine
+    dev = dist.local_rank
+    torch.cuda.set_device(dev)
+    t0 = time.perf_counter()
+    g = load_graph(a.graph, dist)
+    build_s = time.perf_counter() - t0
+    n, m = g.num_nodes, g.num_edges_directed
+    eng = PageRankEngine(dev)
+    t0 = time.perf_counter()
+    eng.upload(g)
+    upload_s = time.perf_counter() - t0
+    upload_bytes = 4 * (n + 1) + 4 * m
+    stream = torch.cuda.current_stream(dev)
+    eng.set_stream(stream.cuda_stream)
+    out = torch.empty(n, dtype=torch.float32, device=f"cuda:{dev}")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")  # 256 MB > L2
+
+    # ---- device-resident solves (value)
+    for _ in range(a.warmup):
+        eng.run_device(a.max_iters, a.epsilon, 0.85, 1, None, out.data_ptr())
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(a.steps)]
+    sweeps_total, sweep_ms_total, launches = 0, 0.0, 0
+    torch.cuda.synchronize()
+    for i in range(a.steps):
+        flush.fill_(float(i))                      # evict L2 between steps
+        ev[i][0].record(stream)
+        sw, _ = eng.run_device(a.max_iters, a.epsilon, 0.85, 1, None, out.data_ptr())
+        ev[i][1].record(stream)
+        sweep_ms, _total_ms, nl = eng.last_timing()
+        sweeps_total += int(sw[0])
+        sweep_ms_total += sweep_ms
+        launches += nl
+    torch.cuda.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in ev]
+    clk = clocks.stop()
+    local_ms = float(sum(step_ms))
+    dist.barrier()
+    max_ms = dist.max(local_ms)
+    sweeps_per_step = sweeps_total / a.steps
+    edges_all = dist.sum(float(m) * sweeps_total)
+    value = edges_all / (max_ms / 1e3) / 1e9
+
+    # ---- end to end through the C-ABI host call (pinned host result buffer)
+    eng.set_stream(None)
+    host_out = torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
+    for _ in range(max(1, a.warmup)):
+        eng.run(a.max_iters, a.epsilon, out=host_out)
+    dist.barrier()
+    e2e_s, e2e_sweeps = 0.0, 0
+    for i in range(a.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = eng.run(a.max_iters, a.epsilon, out=host_out)
+        e2e_s += time.perf_counter() - t0
+        e2e_sweeps += int(res.sweeps[0])
+        launches_e2e = eng.last_timing()[2]
+    e2e_s = dist.max(e2e_s)
+    e2e_edges = dist.sum(float(m) * e2e_sweeps)
+    e2e_value = e2e_edges / e2e_s / 1e9
+
+    # ---- roofline of the fused sweep kernel
+    peak, peak_src = measured_peak()
+    bps = sweep_bytes(n, m, g.directed)
+    avg_sweep_ms = sweep_ms_total / max(sweeps_total, 1)
+    achieved = bps / (avg_sweep_ms / 1e3) / 1e9
+    traffic = profiled_traffic(a.graph)
+
+    result = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "GTEPS",
+        "n_gpus": dist.world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": round(max_ms / a.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (reference generator, identical graph)",
+        "config": {
+            "workload": f"PageRankPull {a.graph.strip()} (Kronecker/uniform per pr_spmv options), "
+                        f"damping 0.85, epsilon {a.epsilon}, max_iters {a.max_iters}",
+            "num_nodes": n, "num_edges_directed": m, "sweeps_per_step": sweeps_per_step,
+            "l2": "256 MB buffer written between steps; graph 4M+4N bytes >> 126 MB L2",
+            "parallelism": f"replicas{dist.world}" if dist.world > 1 else "single GPU",
+            "graph_build_s": round(build_s, 2),
+        },
+        "e2e": {
+            "value": round(e2e_value, 3), "unit": "GTEPS",
+            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4 * n,
+            "path": "pr_gpu_run (C ABI, host scores buffer, pinned)",
+            "upload_once_s": round(upload_s, 3), "upload_once_bytes": upload_bytes,
+            "ms_per_step": round(e2e_s * 1e3 / a.steps, 4),
+        },
+        "roofline": {
+            "kernel": "pull_sweep_kernel",
+            "bound": "hbm",
+            "achieved": round(achieved, 1),
+            "peak": peak,
+            "peak_source": peak_src,
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "traffic": traffic,
+            "algorithmic_bytes_per_sweep": bps,
+            "avg_sweep_ms": round(avg_sweep_ms, 4),
+        },
+        "clocks": clk,
+        "gpu_launches": int(launches),
+    }
+    del flush
+
+    # ---- batched PPR vs sequential single-vector solves (rank 0, N=1 config)
+    if not a.no_ppr and dist.rank == 0:
+        result["ppr"] = run_ppr(a, dev)
+
+    # ---- CPU baseline on this host (rank 0 at N=1 only)
+    if not a.no_cpu_baseline and dist.rank == 0 and dist.world == 1:
+        result["cpu_baseline"] = cpu_baseline(g, a, sweeps_per_step)
+    eng.close()
+    return result
+
+
+def run_ppr(a, dev):
+    import torch
+    from gapbs_b200 import PageRankEngine
+    from gapbs_b200.graph import make_graph
+    g = make_graph(a.ppr_graph)
+    n, m = g.num_nodes, g.num_edges_directed
+    T, sizes = ppr_teleports(g, a.ppr_cols, seed=27491095 + 1)
+    eng = PageRankEngine(dev)
+    eng.upload(g)
+    stream = torch.cuda.current_stream(dev)
+    eng.set_stream(stream.cuda_stream)
+    Td = torch.from_numpy(T).to(f"cuda:{dev}")
+    out = torch.empty_like(Td)
+    cols = [torch.from_numpy(np.ascontiguousarray(T[:, c])).to(f"cuda:{dev}")
+            for c in range(a.ppr_cols)]
+    out1 = torch.empty(n, dtype=torch.float32, device=f"cuda:{dev}")
+    reps = max(1, min(a.steps, 3))
+    # batched
+    for _ in range(max(1, a.warmup)):
+        eng.run_device(a.max_iters, a.epsilon, 0.85, a.ppr_cols, Td.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    bsweeps = None
+    for _ in range(reps):
+        bsweeps, _ = eng.run_device(a.max_iters, a.epsilon, 0.85, a.ppr_cols, Td.data_ptr(),
+                                    out.data_ptr())
+    e.record(stream)
+    torch.cuda.synchronize()
+    b_ms = s.elapsed_time(e) / reps
+    b_gteps = float(m) * float(bsweeps.sum()) / (b_ms / 1e3) / 1e9
+    # sequential single-vector solves
+    for c in range(min(2, a.ppr_cols)):
+        eng.run_device(a.max_iters, a.epsilon, 0.85, 1, cols[c].data_ptr(), out1.data_ptr())
+    torch.cuda.synchronize()
+    s.record(stream)
+    ssweeps = 0
+    for c in range(a.ppr_cols):
+        sw, _ = eng.run_device(a.max_iters, a.epsilon, 0.85, 1, cols[c].data_ptr(), out1.data_ptr())
+        ssweeps += int(sw[0])
+    e.record(stream)
+    torch.cuda.synchronize()
+    s_ms = s.elapsed_time(e)
+    s_gteps = float(m) * ssweeps / (s_ms / 1e3) / 1e9
+    # agreement of the two paths (same columns, same tolerance)
+    maxdiff = 0.0
+    for c in range(0, a.ppr_cols, max(1, a.ppr_cols // 8)):
+        eng.run_device(a.max_iters, a.epsilon, 0.85, 1, cols[c].data_ptr(), out1.data_ptr())
+        maxdiff = max(maxdiff, float((out[:, c] - out1).abs().sum()))
+    eng.close()
+    return {
+        "workload": f"{a.ppr_cols} PPR vectors on {a.ppr_graph.strip()} (N={n}, M={m}), seed sets "
+                    f"log-uniform in [1,4096] (sizes min {min(sizes)} max {max(sizes)})",
+        "batched_gteps": round(b_gteps, 3),
+        "batched_ms": round(b_ms, 3),
+        "batched_sweeps_total": int(bsweeps.sum()),
+        "sequential_gteps": round(s_gteps, 3),
+        "sequential_ms": round(s_ms, 3),
+        "sequential_sweeps_total": ssweeps,
+        "speedup_aggregate_gteps": round(b_gteps / s_gteps, 3),
+        "max_l1_batched_vs_single": maxdiff,
+    }
+
+
+def cpu_baseline(g, a, gpu_sweeps):
+    import oracle
+    cores = os.cpu_count() or 1
+    n, m = g.num_nodes, g.num_edges_directed
+    if oracle.ref_available():
+        rg = oracle.RefGraph.from_csr(g)
+        tot, per = rg.time_pagerank_pull(trials=a.cpu_trials, max_iters=a.max_iters,
+                                         epsilon=a.epsilon)
+        sweeps = gpu_sweeps
+        sec = float(np.mean(per))
+        return {"value": round(m * sweeps / sec / 1e9, 4), "unit": "GTEPS", "cores": cores,
+                "kind": "reference",
+                "sample": f"{a.cpu_trials} full PageRankPull solves of the same graph "
+                          f"({sweeps:.0f} sweeps each) by the reference compiled from source, "
+                          f"OpenMP on {cores} threads; {sec:.3f} s per solve"}
+    # port: single-threaded FP32 oracle, 2 sweeps
+    t0 = time.perf_counter()
+    _, k, _ = oracle.pr_pull_f32(g, max_iters=2, epsilon=0.0)
+    sec = time.perf_counter() - t0
+    return {"value": round(m * k / sec / 1e9, 4), "unit": "GTEPS", "cores": 1, "kind": "port",
+            "sample": f"2 sweeps of the FP32 restatement, one thread, {sec:.3f} s"}
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+
+def capture_fd1(fn, *args):
+    sys.stdout.flush()
+    saved = os.dup(1)
+    with tempfile.TemporaryFile(mode="w+b") as tmp:
+        os.dup2(tmp.fileno(), 1)
+        try:
+            ret = fn(*args)
+        finally:
+            sys.stdout.flush()
+            os.dup2(saved, 1)
+            os.close(saved)
+        tmp.seek(0)
+        return ret, tmp.read().decode()
+
+
+def run_reference(a, dist: Dist):
+    if dist.rank != 0:
+        return None
+    import oracle
+    cores = os.cpu_count() or 1
+    if not oracle.ref_available():
+        # the oracle port stands in (single-threaded FP32 restatement)
+        from gapbs_b200.graph import make_graph
+        g = make_graph(a.graph)
+        m = g.num_edges_directed
+        per = []
+        for i in range(a.warmup + a.steps):
+            t0 = time.perf_counter()
+            _, k, _ = oracle.pr_pull_f32(g, max_iters=2, epsilon=0.0)
+            if i >= a.warmup:
+                per.append((time.perf_counter() - t0, k))
+        sec = sum(p[0] for p in per)
+        val = m * sum(p[1] for p in per) / sec / 1e9
+        kind, sample, cores_used = "port", "2 sweeps per step, FP32 restatement, one thread", 1
+    else:
+        rg, _ = capture_fd1(oracle.RefGraph.build, a.graph)
+        m = rg.num_edges_directed
+        s, log = capture_fd1(rg.pagerank_pull, a.max_iters, a.epsilon, True)
+        sweeps = len([ln for ln in log.splitlines() if ln.strip()])
+        for _ in range(a.warmup):
+            rg.time_pagerank_pull(trials=1, max_iters=a.max_iters, epsilon=a.epsilon)
+        tot, per = rg.time_pagerank_pull(trials=a.steps, max_iters=a.max_iters, epsilon=a.epsilon)
+        val = m * sweeps * a.steps / tot / 1e9
+        kind, cores_used = "reference", cores
+        sample = (f"each step one full PageRankPull solve ({sweeps} sweeps) of {a.graph.strip()} "
+                  f"by the reference compiled from source, OpenMP on {cores} threads")
+    out = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(val, 4),
+        "unit": "GTEPS",
+        "n_gpus": dist.world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (reference generator)",
+        "config": {"workload": f"PageRankPull {a.graph.strip()}, damping 0.85, epsilon "
+                               f"{a.epsilon}, max_iters {a.max_iters}"},
+        "cpu_baseline": {"value": round(val, 4), "unit": "GTEPS", "cores": cores_used,
+                         "kind": kind, "sample": sample},
+        "e2e": {"value": round(val, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    return out
+
+
+def main():
+    a = parse_args()
+    # The reference arm runs on rank 0 alone and needs no process group.
+    dist = Dist(init=a.impl != "reference")
+    try:
+        if a.impl == "reference":
+            res = run_reference(a, dist)
+        else:
+            res = run_ours(a, dist)
+        if dist.rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

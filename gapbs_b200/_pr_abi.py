@@ -1,0 +1,47 @@
+"""ctypes declarations of include/pr_gpu.h (libgapbs_pr.so)."""
+from __future__ import annotations
+
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_void_p
+
+P = c_void_p
+
+PR_GPU_OK = 0
+PR_GPU_EINVAL = -1
+PR_GPU_ECUDA = -2
+PR_GPU_ENOMEM = -3
+PR_GPU_ENOGRAPH = -4
+PR_GPU_EGRAPH = -5
+PR_GPU_ERANGE = -6
+
+# Every symbol include/pr_gpu.h declares.
+SYMBOLS = (
+    "pr_gpu_create", "pr_gpu_upload", "pr_gpu_run", "pr_gpu_run_device",
+    "pr_gpu_adjoint", "pr_gpu_adjoint_device", "pr_gpu_set_stream", "pr_gpu_last_timing",
+    "pr_gpu_graph_info", "pr_gpu_destroy", "pr_gpu_last_error",
+)
+
+
+def declare(lib):
+    lib.pr_gpu_create.argtypes = [POINTER(P), c_int]
+    lib.pr_gpu_create.restype = c_int
+    lib.pr_gpu_upload.argtypes = [P, c_int64, c_int64, P, P, P, P, P]
+    lib.pr_gpu_upload.restype = c_int
+    lib.pr_gpu_run.argtypes = [P, c_int, c_double, c_float, c_int, P, P, P, P]
+    lib.pr_gpu_run.restype = c_int
+    lib.pr_gpu_run_device.argtypes = [P, c_int, c_double, c_float, c_int, P, P, P, P]
+    lib.pr_gpu_run_device.restype = c_int
+    lib.pr_gpu_adjoint.argtypes = [P, c_int, c_double, c_float, P, P, P, P, P]
+    lib.pr_gpu_adjoint.restype = c_int
+    lib.pr_gpu_adjoint_device.argtypes = [P, c_int, c_double, c_float, P, P, P, P, P]
+    lib.pr_gpu_adjoint_device.restype = c_int
+    lib.pr_gpu_set_stream.argtypes = [P, P]
+    lib.pr_gpu_set_stream.restype = c_int
+    lib.pr_gpu_last_timing.argtypes = [P, POINTER(c_double), POINTER(c_double), POINTER(c_int64)]
+    lib.pr_gpu_last_timing.restype = c_int
+    lib.pr_gpu_graph_info.argtypes = [P, POINTER(c_int64), POINTER(c_int64), POINTER(c_int64),
+                                      POINTER(c_int64), c_int]
+    lib.pr_gpu_graph_info.restype = c_int
+    lib.pr_gpu_destroy.argtypes = [P]
+    lib.pr_gpu_destroy.restype = None
+    lib.pr_gpu_last_error.argtypes = [P]
+    lib.pr_gpu_last_error.restype = c_char_p

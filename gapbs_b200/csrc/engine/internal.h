@@ -1,0 +1,174 @@
+// internal.h -- device data layout and launch plumbing shared by the engine's
+// translation units.  Not part of the public ABI (include/pr_gpu.h is).
+//
+// Device mirror of a graph (all arrays in HBM, built once per upload):
+//   Vertices are renumbered by descending in-degree (ties by original id):
+//   perm[new] = old, inv[old] = new.  Row u of the renumbered in-CSR holds
+//   the in-neighbours of perm[u], translated to new ids, in their original
+//   order.  Rows of equal length class are therefore contiguous, which makes
+//   every vertex bin a plain row range, and the most-gathered contrib entries
+//   (the hubs) a dense prefix of the contrib array that stays in L2.
+#ifndef GAPBS_B200_ENGINE_INTERNAL_H_
+#define GAPBS_B200_ENGINE_INTERNAL_H_
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace prgpu {
+
+// Vertex bins, in row order (rows sorted by descending length):
+//   0 HUB   rows of >= hub_min entries, split into segments of kSegEntries;
+//           one block per segment, the last segment's block finishes the row
+//   1..6    G = 32, 16, 8, 4, 2, 1 lanes per row (one row per lane group)
+//   7 ZERO  rows without in-neighbours
+constexpr int kNumBins = 8;
+constexpr int kBinHub = 0;
+constexpr int kBinZero = 7;
+constexpr int kSweepThreads = 256;
+constexpr int kSegEntries = 8192;
+constexpr int kZeroRowsPerThread = 4;
+// Lane-group size of bins 1..6.
+constexpr int kBinGroup[kNumBins] = {kSweepThreads, 32, 16, 8, 4, 2, 1, 1};
+// Grid reduction: stage-1 groups of this many blocks.
+constexpr int kReduceGroup = 512;
+
+// Default minimum row length of each bin (bin b takes rows with
+// length >= min_len[b] not taken by an earlier bin).
+struct BinConfig {
+  int min_len[kNumBins] = {4096, 128, 64, 32, 16, 8, 1, 0};
+};
+
+struct DeviceGraph {
+  int64_t n = 0, m = 0;
+  bool directed = false;
+  bool weighted = false;
+  int64_t max_degree = 0;
+  // renumbered in-CSR
+  int32_t *rowoff = nullptr;   // n+1
+  int32_t *col = nullptr;      // m rounded up to a multiple of 4
+  float *win = nullptr;        // weighted: w(v->u) aligned with col
+  // out-direction data in new ids
+  int32_t *odeg = nullptr;     // directed: out-degree per new id
+  float *rsum = nullptr;       // weighted: S_v = sum of out-weights per new id
+  int32_t *orowoff = nullptr;  // directed: renumbered out-CSR (adjoint)
+  int32_t *ocol = nullptr;
+  float *wout = nullptr;       // weighted: w(v->u) aligned with the out rows
+  int32_t *orig_out_off = nullptr;  // the caller's out-offsets (original ids):
+                                    // entry j of renumbered out-row v sits at
+                                    // orig_out_off[perm[v]] + j in the caller's CSR
+  int32_t *perm = nullptr;     // new -> old
+  int32_t *inv = nullptr;      // old -> new
+  // bins
+  BinConfig bins;
+  int64_t bin_row_start[kNumBins + 1] = {};
+  int64_t num_hub_rows = 0;
+  int64_t num_segments = 0;
+  int32_t *seg_row = nullptr;     // segment -> hub row
+  int32_t *seg_first = nullptr;   // hub row -> first segment (num_hub_rows+1)
+  unsigned *hub_ticket = nullptr; // per hub row
+  float *seg_partial = nullptr;   // per segment
+};
+
+// Per-sweep convergence control, in device memory.
+struct SweepCtl {
+  int done;
+  int sweeps;
+  unsigned tick2;
+  int pad;
+};
+
+struct Scratch {
+  float *score = nullptr;      // n x ncols (new ids)
+  float *contrib[2] = {nullptr, nullptr};
+  float *base = nullptr;       // per-vertex (1-d) t (PPR), new ids
+  float *outbuf = nullptr;     // n x ncols scores in original ids
+  float *tele = nullptr;       // teleport staging (original ids)
+  float *aux[2] = {nullptr, nullptr};  // adjoint: forward scores (new ids), staging
+  float *edge_buf = nullptr;   // adjoint: m edge gradients (device staging)
+  double *norm = nullptr;      // adjoint: ||w||_1
+  int64_t cap_edges = 0;
+  double *part1 = nullptr;     // per block
+  double *part2 = nullptr;     // per stage-1 group
+  unsigned *tick1 = nullptr;   // per stage-1 group
+  double *trace = nullptr;     // max_iters
+  SweepCtl *ctl = nullptr;
+  int64_t cap_n = 0, cap_blocks = 0, cap_iters = 0, cap_cols = 0;
+};
+
+// What one pull sweep computes per row u (sum = gathered neighbour values):
+//   kKindPlain    new = base + d * sum, base a scalar (the reference's PR)
+//   kKindPPR      new = base[u] + d * sum          (personalized PR)
+//   kKindAdjoint  new = base[u] + d * sum / S_u, and the gathered value of u
+//                 is new itself (adjoint iteration over out-rows)
+constexpr int kKindPlain = 0;
+constexpr int kKindPPR = 1;
+constexpr int kKindAdjoint = 2;
+
+// Kernel-side view of one plain / single-column sweep.
+struct PullArgs {
+  int32_t n;
+  int32_t kind;
+  const int32_t *__restrict__ rowoff;
+  const int32_t *__restrict__ col;
+  const float *__restrict__ win;
+  const int32_t *__restrict__ odeg;
+  const float *__restrict__ rsum;
+  const float *__restrict__ base_vec;  // nullptr => base_scalar
+  float base_scalar;
+  float damping;
+  float *score;
+  const float *__restrict__ cin;
+  float *cout;
+  // bins: first block index and first row of each bin
+  int32_t bin_block[kNumBins + 1];
+  int32_t bin_row[kNumBins + 1];
+  const int32_t *__restrict__ seg_row;
+  const int32_t *__restrict__ seg_first;
+  unsigned *hub_ticket;
+  float *seg_partial;
+  // grid reduction
+  double *part1;
+  double *part2;
+  unsigned *tick1;
+  double *trace;
+  SweepCtl *ctl;
+  int32_t nblocks;
+  int32_t iter;
+  double epsilon;
+};
+
+// Launchers (kernels.cu / prep.cu).
+cudaError_t BuildDeviceGraph(DeviceGraph *g, int64_t n, int64_t m,
+                             const int32_t *d_out_off, const int32_t *d_out_nbr,
+                             const int32_t *d_in_off, const int32_t *d_in_nbr,
+                             const float *d_ew, bool directed,
+                             cudaStream_t s, std::string *err);
+void FreeDeviceGraph(DeviceGraph *g);
+
+int PullBlocks(const DeviceGraph &g, int32_t bin_block[kNumBins + 1]);
+
+cudaError_t LaunchPullInit(const DeviceGraph &g, Scratch &sc, const float *tele_new,
+                           float init_scalar, float damping, cudaStream_t s);
+cudaError_t LaunchPullSweep(const PullArgs &a, cudaStream_t s);
+// Warp-per-row sweep over an arbitrary (unsorted) CSR given in a.rowoff /
+// a.col, a.nblocks blocks, grid-stride; used for adjoint sweeps over the
+// out-rows of directed graphs.
+cudaError_t LaunchPullGeneric(const PullArgs &a, cudaStream_t s);
+// Per-edge weight gradient and teleport gradient of the adjoint (pull.cu).
+cudaError_t LaunchAdjointGrads(const DeviceGraph &g, const int32_t *orow, const int32_t *ocol,
+                               const float *wout, const float *lam_new, const float *s_new,
+                               float damping, float *grad_ew, float *grad_t_old,
+                               cudaStream_t s);
+cudaError_t LaunchL1Norm(const float *x, int64_t n, double *out, cudaStream_t s);
+cudaError_t LaunchGatherOut(const DeviceGraph &g, const float *src_new, float *dst_old,
+                            int ncols, cudaStream_t s);
+cudaError_t LaunchScatterIn(const DeviceGraph &g, const float *src_old, float *dst_new,
+                            int ncols, cudaStream_t s);
+cudaError_t LaunchResetCtl(Scratch &sc, int nblocks, int iters, cudaStream_t s);
+
+}  // namespace prgpu
+
+#endif  // GAPBS_B200_ENGINE_INTERNAL_H_

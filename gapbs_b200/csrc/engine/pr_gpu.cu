@@ -1,0 +1,575 @@
+// pr_gpu.cu -- the C ABI (include/pr_gpu.h): handle, upload, solve.
+#include "pr_gpu.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "internal.h"
+#include "batched.h"
+
+using prgpu::DeviceGraph;
+using prgpu::Scratch;
+
+struct pr_gpu {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream in use
+  cudaStream_t own_stream = nullptr;  // created by pr_gpu_create
+  std::string err;
+  DeviceGraph g;
+  bool has_graph = false;
+  Scratch sc;
+  prgpu::BatchScratch bsc;
+  cudaEvent_t ev[4] = {};
+  double last_sweep_ms = 0, last_total_ms = 0;
+  int64_t last_launches = 0;
+  int last_adjoint_sweeps = 0;
+  // pinned staging for host <-> device copies
+  static constexpr size_t kChunk = 32u << 20;
+  void *pinned[2] = {nullptr, nullptr};
+  cudaEvent_t pin_ev[2] = {};
+};
+
+namespace {
+
+int SetErr(pr_gpu_t *h, int code, const std::string &msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int CudaErr(pr_gpu_t *h, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return PR_GPU_OK;
+  const int code = (e == cudaErrorMemoryAllocation) ? PR_GPU_ENOMEM : PR_GPU_ECUDA;
+  return SetErr(h, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define PR_CHECK(h, expr)                                   \
+  do {                                                      \
+    cudaError_t e_ = (expr);                                \
+    if (e_ != cudaSuccess) return CudaErr((h), e_, #expr);  \
+  } while (0)
+
+// Parallel memcpy for large host-to-host staging copies.
+void HostCopy(void *dst, const void *src, size_t bytes) {
+  const size_t kPar = 8u << 20;
+  if (bytes < kPar) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const int nt = 4;
+  std::thread th[nt];
+  const size_t per = (bytes + nt - 1) / nt;
+  for (int t = 0; t < nt; t++) {
+    const size_t lo = std::min(bytes, per * t), hi = std::min(bytes, per * (t + 1));
+    th[t] = std::thread([=] {
+      std::memcpy(static_cast<char *>(dst) + lo, static_cast<const char *>(src) + lo, hi - lo);
+    });
+  }
+  for (auto &x : th) x.join();
+}
+
+int EnsurePinned(pr_gpu_t *h) {
+  for (int i = 0; i < 2; i++) {
+    if (!h->pinned[i]) {
+      PR_CHECK(h, cudaMallocHost(&h->pinned[i], pr_gpu::kChunk));
+      PR_CHECK(h, cudaEventCreateWithFlags(&h->pin_ev[i], cudaEventDisableTiming));
+    }
+  }
+  return PR_GPU_OK;
+}
+
+// Host -> device through two pinned chunks (host copy of chunk k+1 overlaps
+// the DMA of chunk k).
+int CopyToDevice(pr_gpu_t *h, void *dst, const void *src, size_t bytes) {
+  if (bytes == 0) return PR_GPU_OK;
+  int rc = EnsurePinned(h);
+  if (rc) return rc;
+  size_t off = 0;
+  int k = 0;
+  while (off < bytes) {
+    const size_t len = std::min(pr_gpu::kChunk, bytes - off);
+    PR_CHECK(h, cudaEventSynchronize(h->pin_ev[k]));
+    HostCopy(h->pinned[k], static_cast<const char *>(src) + off, len);
+    PR_CHECK(h, cudaMemcpyAsync(static_cast<char *>(dst) + off, h->pinned[k], len,
+                                cudaMemcpyHostToDevice, h->stream));
+    PR_CHECK(h, cudaEventRecord(h->pin_ev[k], h->stream));
+    off += len;
+    k ^= 1;
+  }
+  PR_CHECK(h, cudaStreamSynchronize(h->stream));
+  return PR_GPU_OK;
+}
+
+// Device -> host through the pinned chunks.
+int CopyToHost(pr_gpu_t *h, void *dst, const void *src, size_t bytes) {
+  if (bytes == 0) return PR_GPU_OK;
+  int rc = EnsurePinned(h);
+  if (rc) return rc;
+  size_t off = 0, pend_off = 0, pend_len = 0;
+  int k = 0, pend_k = -1;
+  while (off < bytes) {
+    const size_t len = std::min(pr_gpu::kChunk, bytes - off);
+    PR_CHECK(h, cudaMemcpyAsync(h->pinned[k], static_cast<const char *>(src) + off, len,
+                                cudaMemcpyDeviceToHost, h->stream));
+    PR_CHECK(h, cudaEventRecord(h->pin_ev[k], h->stream));
+    if (pend_k >= 0) {
+      PR_CHECK(h, cudaEventSynchronize(h->pin_ev[pend_k]));
+      HostCopy(static_cast<char *>(dst) + pend_off, h->pinned[pend_k], pend_len);
+    }
+    pend_k = k;
+    pend_off = off;
+    pend_len = len;
+    off += len;
+    k ^= 1;
+  }
+  PR_CHECK(h, cudaEventSynchronize(h->pin_ev[pend_k]));
+  HostCopy(static_cast<char *>(dst) + pend_off, h->pinned[pend_k], pend_len);
+  return PR_GPU_OK;
+}
+
+template <typename T>
+cudaError_t Grow(T **p, int64_t *cap, int64_t need) {
+  if (*p && *cap >= need) return cudaSuccess;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * std::max<int64_t>(need, 1));
+  if (e == cudaSuccess) *cap = need;
+  return e;
+}
+
+void FreeScratch(Scratch *sc) {
+  void *ptrs[] = {sc->score, sc->contrib[0], sc->contrib[1], sc->base, sc->outbuf, sc->tele,
+                  sc->aux[0], sc->aux[1], sc->edge_buf, sc->norm,
+                  sc->part1, sc->part2, sc->tick1, sc->trace, sc->ctl};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  *sc = Scratch();
+}
+
+// Scratch for an n-vertex, ncols-column solve of nblocks blocks and iters sweeps.
+int EnsureScratch(pr_gpu_t *h, int64_t n, int ncols, int64_t nblocks, int iters) {
+  Scratch &s = h->sc;
+  const int64_t cells = n * ncols;
+  if (!s.score || s.cap_n < cells) {
+    for (float **p : {&s.score, &s.contrib[0], &s.contrib[1], &s.base, &s.outbuf, &s.tele,
+                      &s.aux[0], &s.aux[1]}) {
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+    }
+    s.cap_n = 0;
+    for (float **p : {&s.score, &s.contrib[0], &s.contrib[1], &s.base, &s.outbuf, &s.tele,
+                      &s.aux[0], &s.aux[1]})
+      PR_CHECK(h, cudaMalloc(p, sizeof(float) * std::max<int64_t>(cells, 1)));
+    s.cap_n = cells;
+  }
+  int64_t cap = s.cap_blocks;
+  const int64_t ngroups = (nblocks + prgpu::kReduceGroup - 1) / prgpu::kReduceGroup;
+  if (!s.part1 || cap < nblocks) {
+    int64_t c1 = 0, c2 = 0, c3 = 0;
+    if (s.part1) cudaFree(s.part1), s.part1 = nullptr;
+    if (s.part2) cudaFree(s.part2), s.part2 = nullptr;
+    if (s.tick1) cudaFree(s.tick1), s.tick1 = nullptr;
+    PR_CHECK(h, Grow(&s.part1, &c1, nblocks));
+    PR_CHECK(h, Grow(&s.part2, &c2, ngroups + 1));
+    PR_CHECK(h, Grow(&s.tick1, &c3, ngroups + 1));
+    s.cap_blocks = nblocks;
+  }
+  PR_CHECK(h, Grow(&s.trace, &s.cap_iters, std::max(iters, 1)));
+  if (!s.ctl) PR_CHECK(h, cudaMalloc(&s.ctl, sizeof(prgpu::SweepCtl)));
+  if (!s.norm) PR_CHECK(h, cudaMalloc(&s.norm, sizeof(double)));
+  return PR_GPU_OK;
+}
+
+int CheckRunArgs(pr_gpu_t *h, int max_iters, int ncols) {
+  if (!h) return PR_GPU_EINVAL;
+  if (!h->has_graph) return SetErr(h, PR_GPU_ENOGRAPH, "no graph uploaded");
+  if (max_iters < 0) return SetErr(h, PR_GPU_EINVAL, "max_iters must be >= 0");
+  if (ncols < 1) return SetErr(h, PR_GPU_EINVAL, "ncols must be >= 1");
+  return PR_GPU_OK;
+}
+
+// Single-column solve on device buffers.  tele_old: teleport in original ids
+// (device) or nullptr for the reference's uniform PageRank.  out_old: device
+// buffer for scores in original ids.
+int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
+                const float *tele_old, float *out_old, int32_t *sweeps_out, double *err_trace) {
+  DeviceGraph &g = h->g;
+  int32_t bin_block[prgpu::kNumBins + 1];
+  const int nblocks = prgpu::PullBlocks(g, bin_block);
+  int rc = EnsureScratch(h, g.n, 1, nblocks, max_iters);
+  if (rc) return rc;
+  Scratch &sc = h->sc;
+  cudaStream_t s = h->stream;
+  int64_t launches = 0;
+  PR_CHECK(h, cudaEventRecord(h->ev[0], s));
+  const float *tele_new = nullptr;
+  if (tele_old) {
+    PR_CHECK(h, prgpu::LaunchScatterIn(g, tele_old, sc.contrib[1], 1, s));
+    tele_new = sc.contrib[1];
+    launches++;
+  }
+  const float n_f = static_cast<float>(g.n);
+  const float init_score = 1.0f / n_f;                 // src/pr_spmv.cc:37
+  const float base_score = (1.0f - damping) / n_f;     // src/pr_spmv.cc:38
+  PR_CHECK(h, prgpu::LaunchResetCtl(sc, nblocks, max_iters, s));
+  PR_CHECK(h, prgpu::LaunchPullInit(g, sc, tele_new, init_score, damping, s));
+  launches++;
+  prgpu::PullArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n = static_cast<int32_t>(g.n);
+  a.rowoff = g.rowoff;
+  a.col = g.col;
+  a.win = g.weighted ? g.win : nullptr;
+  a.odeg = (g.directed && !g.weighted) ? g.odeg : nullptr;
+  a.rsum = g.weighted ? g.rsum : nullptr;
+  a.kind = tele_old ? prgpu::kKindPPR : prgpu::kKindPlain;
+  a.base_vec = tele_old ? sc.base : nullptr;
+  a.base_scalar = base_score;
+  a.damping = damping;
+  a.score = sc.score;
+  for (int b = 0; b <= prgpu::kNumBins; b++) {
+    a.bin_block[b] = bin_block[b];
+    a.bin_row[b] = static_cast<int32_t>(g.bin_row_start[b]);
+  }
+  a.seg_row = g.seg_row;
+  a.seg_first = g.seg_first;
+  a.hub_ticket = g.hub_ticket;
+  a.seg_partial = g.seg_partial;
+  a.part1 = sc.part1;
+  a.part2 = sc.part2;
+  a.tick1 = sc.tick1;
+  a.trace = sc.trace;
+  a.ctl = sc.ctl;
+  a.nblocks = nblocks;
+  a.epsilon = epsilon;
+  PR_CHECK(h, cudaEventRecord(h->ev[1], s));
+  for (int it = 0; it < max_iters; it++) {
+    a.iter = it;
+    a.cin = sc.contrib[it & 1];
+    a.cout = sc.contrib[(it + 1) & 1];
+    PR_CHECK(h, prgpu::LaunchPullSweep(a, s));
+    launches += nblocks ? 1 : 0;
+  }
+  PR_CHECK(h, cudaEventRecord(h->ev[2], s));
+  PR_CHECK(h, prgpu::LaunchGatherOut(g, sc.score, out_old, 1, s));
+  launches++;
+  PR_CHECK(h, cudaEventRecord(h->ev[3], s));
+  prgpu::SweepCtl ctl;
+  std::vector<double> trace(std::max(max_iters, 1));
+  PR_CHECK(h, cudaMemcpyAsync(&ctl, sc.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+  if (max_iters)
+    PR_CHECK(h, cudaMemcpyAsync(trace.data(), sc.trace, sizeof(double) * max_iters,
+                                cudaMemcpyDeviceToHost, s));
+  PR_CHECK(h, cudaStreamSynchronize(s));
+  float ms_sweep = 0, ms_total = 0;
+  cudaEventElapsedTime(&ms_sweep, h->ev[1], h->ev[2]);
+  cudaEventElapsedTime(&ms_total, h->ev[0], h->ev[3]);
+  h->last_sweep_ms = ms_sweep;
+  h->last_total_ms = ms_total;
+  h->last_launches = launches;
+  if (sweeps_out) *sweeps_out = max_iters ? ctl.sweeps : 0;
+  if (err_trace)
+    for (int i = 0; i < max_iters; i++) err_trace[i] = trace[i];
+  return PR_GPU_OK;
+}
+
+
+// Adjoint solve on device buffers (original ids in, original ids out).
+int SolveAdjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping, const float *w_old,
+                 const float *s_old, float *grad_t_old, float *grad_ew) {
+  DeviceGraph &g = h->g;
+  int32_t bin_block[prgpu::kNumBins + 1];
+  const bool generic = g.directed;
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
+  const int nblocks = generic ? dev_sms * 8 : prgpu::PullBlocks(g, bin_block);
+  int rc = EnsureScratch(h, g.n, 1, nblocks, max_iters);
+  if (rc) return rc;
+  Scratch &sc = h->sc;
+  cudaStream_t s = h->stream;
+  int64_t launches = 0;
+  PR_CHECK(h, cudaEventRecord(h->ev[0], s));
+  // w and s in new ids; lambda_0 = w
+  PR_CHECK(h, prgpu::LaunchScatterIn(g, w_old, sc.base, 1, s));
+  PR_CHECK(h, prgpu::LaunchScatterIn(g, s_old, sc.aux[0], 1, s));
+  PR_CHECK(h, prgpu::LaunchL1Norm(w_old, g.n, sc.norm, s));
+  launches += 3;
+  PR_CHECK(h, cudaMemcpyAsync(sc.score, sc.base, sizeof(float) * g.n, cudaMemcpyDeviceToDevice, s));
+  PR_CHECK(h, cudaMemcpyAsync(sc.contrib[0], sc.base, sizeof(float) * g.n, cudaMemcpyDeviceToDevice, s));
+  double wnorm = 0;
+  PR_CHECK(h, cudaMemcpyAsync(&wnorm, sc.norm, sizeof(double), cudaMemcpyDeviceToHost, s));
+  PR_CHECK(h, cudaStreamSynchronize(s));
+  PR_CHECK(h, prgpu::LaunchResetCtl(sc, nblocks, max_iters, s));
+  const int32_t *orow = generic ? g.orowoff : g.rowoff;
+  const int32_t *ocol = generic ? g.ocol : g.col;
+  prgpu::PullArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n = static_cast<int32_t>(g.n);
+  a.kind = prgpu::kKindAdjoint;
+  a.rowoff = orow;
+  a.col = ocol;
+  a.win = g.weighted ? g.wout : nullptr;
+  a.odeg = nullptr;
+  a.rsum = g.weighted ? g.rsum : nullptr;
+  a.base_vec = sc.base;
+  a.damping = damping;
+  a.score = sc.score;
+  if (!generic) {
+    for (int b = 0; b <= prgpu::kNumBins; b++) {
+      a.bin_block[b] = bin_block[b];
+      a.bin_row[b] = static_cast<int32_t>(g.bin_row_start[b]);
+    }
+    a.seg_row = g.seg_row;
+    a.seg_first = g.seg_first;
+    a.hub_ticket = g.hub_ticket;
+    a.seg_partial = g.seg_partial;
+  }
+  a.part1 = sc.part1;
+  a.part2 = sc.part2;
+  a.tick1 = sc.tick1;
+  a.trace = sc.trace;
+  a.ctl = sc.ctl;
+  a.nblocks = nblocks;
+  a.epsilon = epsilon * wnorm;
+  PR_CHECK(h, cudaEventRecord(h->ev[1], s));
+  for (int it = 0; it < max_iters; it++) {
+    a.iter = it;
+    a.cin = sc.contrib[it & 1];
+    a.cout = sc.contrib[(it + 1) & 1];
+    PR_CHECK(h, generic ? prgpu::LaunchPullGeneric(a, s) : prgpu::LaunchPullSweep(a, s));
+    launches++;
+  }
+  PR_CHECK(h, cudaEventRecord(h->ev[2], s));
+  PR_CHECK(h, prgpu::LaunchAdjointGrads(g, orow, ocol, g.weighted ? g.wout : nullptr, sc.score,
+                                        sc.aux[0], damping, grad_ew, grad_t_old, s));
+  launches += 2;
+  PR_CHECK(h, cudaEventRecord(h->ev[3], s));
+  prgpu::SweepCtl ctl;
+  PR_CHECK(h, cudaMemcpyAsync(&ctl, sc.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+  PR_CHECK(h, cudaStreamSynchronize(s));
+  float ms_sweep = 0, ms_total = 0;
+  cudaEventElapsedTime(&ms_sweep, h->ev[1], h->ev[2]);
+  cudaEventElapsedTime(&ms_total, h->ev[0], h->ev[3]);
+  h->last_sweep_ms = ms_sweep;
+  h->last_total_ms = ms_total;
+  h->last_launches = launches;
+  h->last_adjoint_sweeps = max_iters ? ctl.sweeps : 0;
+  return PR_GPU_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int pr_gpu_create(pr_gpu_t **out, int device) {
+  if (!out) return PR_GPU_EINVAL;
+  *out = nullptr;
+  pr_gpu_t *h = new (std::nothrow) pr_gpu();
+  if (!h) return PR_GPU_ENOMEM;
+  h->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+  h->stream = h->own_stream;
+  for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&h->ev[i]);
+  if (e != cudaSuccess) {
+    delete h;
+    return PR_GPU_ECUDA;
+  }
+  *out = h;
+  return PR_GPU_OK;
+}
+
+void pr_gpu_destroy(pr_gpu_t *h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  prgpu::FreeDeviceGraph(&h->g);
+  FreeScratch(&h->sc);
+  prgpu::FreeBatchScratch(&h->bsc);
+  for (int i = 0; i < 2; i++) {
+    if (h->pinned[i]) cudaFreeHost(h->pinned[i]);
+    if (h->pin_ev[i]) cudaEventDestroy(h->pin_ev[i]);
+  }
+  for (auto &e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+}
+
+const char *pr_gpu_last_error(const pr_gpu_t *h) {
+  return h ? h->err.c_str() : "invalid handle";
+}
+
+int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m, const int32_t *out_off,
+                  const int32_t *out_nbr, const int32_t *in_off, const int32_t *in_nbr,
+                  const float *edge_w) {
+  if (!h) return PR_GPU_EINVAL;
+  if (n < 1 || m < 0) return SetErr(h, PR_GPU_EINVAL, "need n >= 1 and m >= 0");
+  if (n > 0x7fffffffLL - 1 || m > 0x7fffffffLL - 8)
+    return SetErr(h, PR_GPU_ERANGE, "graph exceeds int32 ids / offsets");
+  if (!out_off || (m > 0 && !out_nbr)) return SetErr(h, PR_GPU_EINVAL, "null CSR array");
+  const bool directed = in_off && (in_off != out_off || in_nbr != out_nbr);
+  if (directed && m > 0 && !in_nbr) return SetErr(h, PR_GPU_EINVAL, "null in-CSR array");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  h->has_graph = false;
+  prgpu::FreeDeviceGraph(&h->g);
+  int32_t *d_oo = nullptr, *d_on = nullptr, *d_io = nullptr, *d_in = nullptr;
+  float *d_w = nullptr;
+  auto release = [&]() {
+    for (void *p : {static_cast<void *>(d_oo), static_cast<void *>(d_on),
+                    static_cast<void *>(d_io), static_cast<void *>(d_in),
+                    static_cast<void *>(d_w)})
+      if (p) cudaFree(p);
+  };
+  cudaError_t e = cudaMalloc(&d_oo, sizeof(int32_t) * (n + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&d_on, sizeof(int32_t) * std::max<int64_t>(m, 1));
+  if (e == cudaSuccess && directed) e = cudaMalloc(&d_io, sizeof(int32_t) * (n + 1));
+  if (e == cudaSuccess && directed) e = cudaMalloc(&d_in, sizeof(int32_t) * std::max<int64_t>(m, 1));
+  if (e == cudaSuccess && edge_w) e = cudaMalloc(&d_w, sizeof(float) * std::max<int64_t>(m, 1));
+  if (e != cudaSuccess) {
+    release();
+    return CudaErr(h, e, "device allocation for upload");
+  }
+  int rc = CopyToDevice(h, d_oo, out_off, sizeof(int32_t) * (n + 1));
+  if (!rc) rc = CopyToDevice(h, d_on, out_nbr, sizeof(int32_t) * m);
+  if (!rc && directed) rc = CopyToDevice(h, d_io, in_off, sizeof(int32_t) * (n + 1));
+  if (!rc && directed) rc = CopyToDevice(h, d_in, in_nbr, sizeof(int32_t) * m);
+  if (!rc && edge_w) rc = CopyToDevice(h, d_w, edge_w, sizeof(float) * m);
+  if (rc) {
+    release();
+    return rc;
+  }
+  std::string msg;
+  e = prgpu::BuildDeviceGraph(&h->g, n, m, d_oo, d_on, directed ? d_io : d_oo,
+                              directed ? d_in : d_on, d_w, directed, h->stream, &msg);
+  release();
+  if (e == cudaErrorInvalidValue && !msg.empty() && msg.rfind("invalid CSR", 0) == 0)
+    return SetErr(h, PR_GPU_EGRAPH, msg);
+  if (e != cudaSuccess) return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
+  h->has_graph = true;
+  return PR_GPU_OK;
+}
+
+int pr_gpu_run_device(pr_gpu_t *h, int max_iters, double epsilon, float damping, int ncols,
+                      const float *teleport_dev, float *scores_out_dev, int32_t *sweeps_out,
+                      double *err_trace) {
+  int rc = CheckRunArgs(h, max_iters, ncols);
+  if (rc) return rc;
+  if (!scores_out_dev) return SetErr(h, PR_GPU_EINVAL, "scores_out is null");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  if (ncols == 1)
+    return SolveSingle(h, max_iters, epsilon, damping, teleport_dev, scores_out_dev, sweeps_out,
+                       err_trace);
+  double ms_sweep = 0, ms_total = 0;
+  int64_t launches = 0;
+  std::string msg;
+  cudaError_t e = prgpu::SolveBatched(h->g, h->bsc, h->stream, max_iters, epsilon, damping,
+                                      ncols, teleport_dev, scores_out_dev, sweeps_out, err_trace,
+                                      &ms_sweep, &ms_total, &launches, &msg);
+  if (e != cudaSuccess)
+    return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
+  h->last_sweep_ms = ms_sweep;
+  h->last_total_ms = ms_total;
+  h->last_launches = launches;
+  return PR_GPU_OK;
+}
+
+int pr_gpu_run(pr_gpu_t *h, int max_iters, double epsilon, float damping, int ncols,
+               const float *teleport, float *scores_out, int32_t *sweeps_out,
+               double *err_trace) {
+  int rc = CheckRunArgs(h, max_iters, ncols);
+  if (rc) return rc;
+  if (!scores_out) return SetErr(h, PR_GPU_EINVAL, "scores_out is null");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  const int64_t cells = h->g.n * ncols;
+  // outbuf / tele live in the single-column scratch; make room for ncols.
+  rc = EnsureScratch(h, h->g.n, ncols, 1, std::max(max_iters, 1));
+  if (rc) return rc;
+  const float *tele_dev = nullptr;
+  if (teleport) {
+    rc = CopyToDevice(h, h->sc.tele, teleport, sizeof(float) * cells);
+    if (rc) return rc;
+    tele_dev = h->sc.tele;
+  }
+  rc = pr_gpu_run_device(h, max_iters, epsilon, damping, ncols, tele_dev, h->sc.outbuf,
+                         sweeps_out, err_trace);
+  if (rc) return rc;
+  return CopyToHost(h, scores_out, h->sc.outbuf, sizeof(float) * cells);
+}
+
+
+int pr_gpu_adjoint_device(pr_gpu_t *h, int max_iters, double epsilon, float damping,
+                          const float *loss_w_dev, const float *scores_dev,
+                          float *grad_teleport_dev, float *grad_edge_w_dev, int32_t *sweeps_out) {
+  int rc = CheckRunArgs(h, max_iters, 1);
+  if (rc) return rc;
+  if (!loss_w_dev || !scores_dev) return SetErr(h, PR_GPU_EINVAL, "loss_w / scores is null");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  rc = SolveAdjoint(h, max_iters, epsilon, damping, loss_w_dev, scores_dev, grad_teleport_dev,
+                    grad_edge_w_dev);
+  if (rc) return rc;
+  if (sweeps_out) *sweeps_out = h->last_adjoint_sweeps;
+  return PR_GPU_OK;
+}
+
+int pr_gpu_adjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping,
+                   const float *loss_w, const float *scores, float *grad_teleport,
+                   float *grad_edge_w, int32_t *sweeps_out) {
+  int rc = CheckRunArgs(h, max_iters, 1);
+  if (rc) return rc;
+  if (!loss_w || !scores) return SetErr(h, PR_GPU_EINVAL, "loss_w / scores is null");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  const int64_t n = h->g.n, m = h->g.m;
+  rc = EnsureScratch(h, n, 1, 1, std::max(max_iters, 1));
+  if (rc) return rc;
+  Scratch &sc = h->sc;
+  if (grad_edge_w) PR_CHECK(h, Grow(&sc.edge_buf, &sc.cap_edges, std::max<int64_t>(m, 1)));
+  rc = CopyToDevice(h, sc.tele, loss_w, sizeof(float) * n);
+  if (!rc) rc = CopyToDevice(h, sc.aux[1], scores, sizeof(float) * n);
+  if (rc) return rc;
+  rc = pr_gpu_adjoint_device(h, max_iters, epsilon, damping, sc.tele, sc.aux[1],
+                             grad_teleport ? sc.outbuf : nullptr,
+                             grad_edge_w ? sc.edge_buf : nullptr, sweeps_out);
+  if (rc) return rc;
+  if (grad_teleport) rc = CopyToHost(h, grad_teleport, sc.outbuf, sizeof(float) * n);
+  if (!rc && grad_edge_w) rc = CopyToHost(h, grad_edge_w, sc.edge_buf, sizeof(float) * m);
+  return rc;
+}
+
+int pr_gpu_set_stream(pr_gpu_t *h, void *stream) {
+  if (!h) return PR_GPU_EINVAL;
+  PR_CHECK(h, cudaSetDevice(h->device));
+  PR_CHECK(h, cudaStreamSynchronize(h->stream));
+  h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+  return PR_GPU_OK;
+}
+
+int pr_gpu_last_timing(const pr_gpu_t *h, double *sweep_ms, double *total_ms,
+                       int64_t *kernel_launches) {
+  if (!h) return PR_GPU_EINVAL;
+  if (sweep_ms) *sweep_ms = h->last_sweep_ms;
+  if (total_ms) *total_ms = h->last_total_ms;
+  if (kernel_launches) *kernel_launches = h->last_launches;
+  return PR_GPU_OK;
+}
+
+int pr_gpu_graph_info(const pr_gpu_t *h, int64_t *n, int64_t *m, int64_t *max_degree,
+                      int64_t *bin_rows, int nbins) {
+  if (!h) return PR_GPU_EINVAL;
+  if (!h->has_graph) return PR_GPU_ENOGRAPH;
+  if (n) *n = h->g.n;
+  if (m) *m = h->g.m;
+  if (max_degree) *max_degree = h->g.max_degree;
+  if (bin_rows)
+    for (int b = 0; b < nbins && b < prgpu::kNumBins; b++)
+      bin_rows[b] = h->g.bin_row_start[b + 1] - h->g.bin_row_start[b];
+  return PR_GPU_OK;
+}
+
+}  // extern "C"

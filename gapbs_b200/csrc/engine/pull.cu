@@ -1,0 +1,505 @@
+// pull.cu -- the fused pull-direction Jacobi sweep (one launch per sweep).
+//
+// One launch performs, for every vertex u, what the reference does in two
+// OpenMP loops plus a reduction (src/pr_spmv.cc:43-54):
+//   sum   = sum over in-neighbours v of contrib[v]
+//   new   = base + d * sum                      (float, two roundings)
+//   err  += |new - old|                          (float difference, FP64 sum)
+//   contrib'[u] = new / out_degree(u)            (next sweep's input)
+// and then decides convergence on the device (error < epsilon, :57-58), so a
+// whole solve is max_iters back-to-back launches with no host round trip; a
+// launch that finds the solve converged returns immediately.
+//
+// Work split (rows are renumbered by descending in-degree, so each bin is a
+// contiguous row range):
+//   HUB   one block per kSegEntries-entry segment of a long row; the block
+//         that finishes a row's last segment (per-row ticket) sums the
+//         segment partials in segment order and updates the row;
+//   G=32..1  lane groups of G threads per row, 128-bit neighbour loads (each
+//         lane reads whole aligned 4-entry chunks and masks entries outside
+//         its row), two chunks in flight per lane, xor-tree group sum;
+//   ZERO  rows without in-neighbours: new = base.
+// The L1 error is reduced in FP64 with a deterministic two-stage tree
+// (per-block partials -> per-512-block group -> total).
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace prgpu {
+
+// The reference's float update: base + d * sum with two roundings (no FMA).
+__device__ __forceinline__ float pr_update(float base, float d, float sum) {
+  return __fadd_rn(base, __fmul_rn(d, sum));
+}
+
+template <bool W>
+__device__ __forceinline__ float gather_chunk(float acc, const int4 q, const float4 w,
+                                              int b, int s, int e, const float *cin,
+                                              uint64_t pg) {
+  const bool i0 = (b >= s) & (b < e);
+  const bool i1 = (b + 1 >= s) & (b + 1 < e);
+  const bool i2 = (b + 2 >= s) & (b + 2 < e);
+  const bool i3 = (b + 3 >= s) & (b + 3 < e);
+  float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
+  if (i0) v0 = ld_gather(cin + q.x, pg);
+  if (i1) v1 = ld_gather(cin + q.y, pg);
+  if (i2) v2 = ld_gather(cin + q.z, pg);
+  if (i3) v3 = ld_gather(cin + q.w, pg);
+  if (W) {
+    if (i0) acc = __fmaf_rn(w.x, v0, acc);
+    if (i1) acc = __fmaf_rn(w.y, v1, acc);
+    if (i2) acc = __fmaf_rn(w.z, v2, acc);
+    if (i3) acc = __fmaf_rn(w.w, v3, acc);
+  } else {
+    if (i0) acc = __fadd_rn(acc, v0);
+    if (i1) acc = __fadd_rn(acc, v1);
+    if (i2) acc = __fadd_rn(acc, v2);
+    if (i3) acc = __fadd_rn(acc, v3);
+  }
+  return acc;
+}
+
+// Sum over entries [s, e) by the calling lane of a G-lane group: the lane
+// takes aligned chunks (s/4 + lane), (s/4 + lane + G), ...; two chunk loads
+// are issued before their gathers.
+template <int G, bool W>
+__device__ __forceinline__ float lane_partial(const PullArgs &a, int s, int e, int lane,
+                                              uint64_t ps, uint64_t pg) {
+  const int4 *col4 = reinterpret_cast<const int4 *>(a.col);
+  const float4 *w4 = reinterpret_cast<const float4 *>(a.win);
+  float acc = 0.f;
+  const int c1 = (e + 3) >> 2;
+  int c = (s >> 2) + lane;
+  for (; c + G < c1; c += 2 * G) {
+    const int4 q0 = ld_stream_v4(col4 + c, ps);
+    const int4 q1 = ld_stream_v4(col4 + c + G, ps);
+    float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f), w1 = w0;
+    if (W) {
+      w0 = ld_stream_v4f(w4 + c, ps);
+      w1 = ld_stream_v4f(w4 + c + G, ps);
+    }
+    acc = gather_chunk<W>(acc, q0, w0, c << 2, s, e, a.cin, pg);
+    acc = gather_chunk<W>(acc, q1, w1, (c + G) << 2, s, e, a.cin, pg);
+  }
+  if (c < c1) {
+    const int4 q0 = ld_stream_v4(col4 + c, ps);
+    float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (W) w0 = ld_stream_v4f(w4 + c, ps);
+    acc = gather_chunk<W>(acc, q0, w0, c << 2, s, e, a.cin, pg);
+  }
+  return acc;
+}
+
+template <bool W, bool DIR>
+__device__ __forceinline__ float denom_of(const PullArgs &a, int u, int s, int e) {
+  if (W) return a.rsum[u];
+  if (DIR) return __int2float_rn(a.odeg[u]);
+  return __int2float_rn(e - s);
+}
+
+// Updates row u from its gathered sum; returns |new - old| (as float).
+template <bool W, bool DIR, int KIND>
+__device__ __forceinline__ float finish_row(const PullArgs &a, int u, int s, int e,
+                                            float sum, uint64_t ps, uint64_t pl) {
+  const float old = ld_score(a.score + u, ps);
+  const float base = KIND != kKindPlain ? a.base_vec[u] : a.base_scalar;
+  if (KIND == kKindAdjoint) {
+    // lambda[v] = w[v] + d * (sum_u w(v->u) lambda[u]) / S_v; lambda itself
+    // is what the next sweep gathers.
+    const float nw = pr_update(base, a.damping, __fdiv_rn(sum, denom_of<W, DIR>(a, u, s, e)));
+    st_hint_f32(a.score + u, nw, ps);
+    st_hint_f32(a.cout + u, nw, pl);
+    return fabsf(__fsub_rn(nw, old));
+  }
+  const float nw = pr_update(base, a.damping, sum);
+  st_hint_f32(a.score + u, nw, ps);
+  st_hint_f32(a.cout + u, __fdiv_rn(nw, denom_of<W, DIR>(a, u, s, e)), pl);
+  return fabsf(__fsub_rn(nw, old));
+}
+
+// Deterministic two-stage FP64 grid reduction of the block errors; the last
+// block records the sweep's error and the convergence decision.
+__device__ __forceinline__ void grid_finish(const PullArgs &a, double block_err,
+                                            double *sred) {
+  __shared__ int s_last;
+  const int b = blockIdx.x;
+  const int g = b / kReduceGroup;
+  const int gsize = min(kReduceGroup, a.nblocks - g * kReduceGroup);
+  const int ngroups = (a.nblocks + kReduceGroup - 1) / kReduceGroup;
+  if (threadIdx.x == 0) {
+    a.part1[b] = block_err;
+    __threadfence();
+    const unsigned t = atomicAdd(&a.tick1[g], 1u);
+    s_last = (t == static_cast<unsigned>(gsize - 1));
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double v = 0;
+  for (int i = threadIdx.x; i < gsize; i += blockDim.x)
+    v += __ldcg(a.part1 + g * kReduceGroup + i);
+  double tot = block_sum_d<kSweepThreads>(v, sred);
+  if (threadIdx.x == 0) {
+    a.part2[g] = tot;
+    a.tick1[g] = 0;
+    __threadfence();
+    const unsigned t2 = atomicAdd(&a.ctl->tick2, 1u);
+    s_last = (t2 == static_cast<unsigned>(ngroups - 1));
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  v = 0;
+  for (int i = threadIdx.x; i < ngroups; i += blockDim.x) v += __ldcg(a.part2 + i);
+  tot = block_sum_d<kSweepThreads>(v, sred);
+  if (threadIdx.x == 0) {
+    a.trace[a.iter] = tot;
+    a.ctl->sweeps = a.iter + 1;
+    a.ctl->tick2 = 0;
+    if (tot < a.epsilon) a.ctl->done = 1;
+    __threadfence();
+  }
+}
+
+template <int G, bool W, bool DIR, int KIND>
+__device__ __forceinline__ float group_rows(const PullArgs &a, int bin, uint64_t ps,
+                                            uint64_t pg, uint64_t pl) {
+  constexpr int kRowsPerBlock = kSweepThreads / G;
+  const int lane = threadIdx.x % G;
+  const int u = a.bin_row[bin] + (blockIdx.x - a.bin_block[bin]) * kRowsPerBlock +
+                static_cast<int>(threadIdx.x) / G;
+  const bool valid = u < a.bin_row[bin + 1];
+  int s = 0, e = 0;
+  if (valid) {
+    s = a.rowoff[u];
+    e = a.rowoff[u + 1];
+  }
+  float acc = lane_partial<G, W>(a, s, e, lane, ps, pg);
+  acc = group_sum<G>(acc);
+  float err = 0.f;
+  if (valid && lane == 0) err = finish_row<W, DIR, KIND>(a, u, s, e, acc, ps, pl);
+  return err;
+}
+
+template <bool W, bool DIR, int KIND>
+__device__ __forceinline__ float hub_segment(const PullArgs &a, float *sredf, uint64_t ps,
+                                             uint64_t pg, uint64_t pl) {
+  __shared__ int s_fin;
+  const int seg = blockIdx.x - a.bin_block[kBinHub];
+  const int u = a.seg_row[seg];
+  const int first = a.seg_first[u];
+  const int nseg = a.seg_first[u + 1] - first;
+  const int rs = a.rowoff[u], re = a.rowoff[u + 1];
+  const int s = rs + (seg - first) * kSegEntries;
+  const int e = min(re, s + kSegEntries);
+  float acc = lane_partial<kSweepThreads, W>(a, s, e, threadIdx.x, ps, pg);
+  const float part = block_sum_f<kSweepThreads>(acc, sredf);
+  if (threadIdx.x == 0) {
+    a.seg_partial[seg] = part;
+    __threadfence();
+    const unsigned t = atomicAdd(a.hub_ticket + u, 1u);
+    s_fin = (t == static_cast<unsigned>(nseg - 1));
+  }
+  __syncthreads();
+  float err = 0.f;
+  if (s_fin && threadIdx.x == 0) {
+    __threadfence();
+    float sum = 0.f;
+    for (int k = 0; k < nseg; k++) sum = __fadd_rn(sum, __ldcg(a.seg_partial + first + k));
+    a.hub_ticket[u] = 0;
+    err = finish_row<W, DIR, KIND>(a, u, rs, re, sum, ps, pl);
+  }
+  return err;
+}
+
+template <bool W, bool DIR, int KIND>
+__device__ __forceinline__ float zero_rows(const PullArgs &a, uint64_t ps, uint64_t pl) {
+  constexpr int kRows = kSweepThreads * kZeroRowsPerThread;
+  const int row0 = a.bin_row[kBinZero] + (blockIdx.x - a.bin_block[kBinZero]) * kRows;
+  const int end = a.bin_row[kBinZero + 1];
+  float err = 0.f;
+#pragma unroll
+  for (int i = 0; i < kZeroRowsPerThread; i++) {
+    const int u = row0 + i * kSweepThreads + threadIdx.x;
+    if (u < end) {
+      const float old = ld_score(a.score + u, ps);
+      const float base = KIND != kKindPlain ? a.base_vec[u] : a.base_scalar;
+      const float nw = pr_update(base, a.damping, 0.f);
+      st_hint_f32(a.score + u, nw, ps);
+      // A row without in-neighbours can still have out-neighbours in a
+      // directed graph; its contrib is then read by the next sweep.
+      if (KIND == kKindAdjoint) st_hint_f32(a.cout + u, nw, pl);
+      else if (W || DIR) st_hint_f32(a.cout + u, __fdiv_rn(nw, denom_of<W, DIR>(a, u, 0, 0)), pl);
+      err += fabsf(__fsub_rn(nw, old));
+    }
+  }
+  return err;
+}
+
+template <bool W, bool DIR, int KIND>
+__global__ void __launch_bounds__(kSweepThreads)
+pull_sweep_kernel(const PullArgs a) {
+  if (*reinterpret_cast<volatile const int *>(&a.ctl->done)) return;
+  __shared__ double sred[kSweepThreads / 32];
+  __shared__ float sredf[kSweepThreads / 32];
+  const uint64_t ps = policy_evict_first();
+  const uint64_t pg = policy_evict_last();
+  const uint64_t pl = pg;
+  const int b = blockIdx.x;
+  int bin = 0;
+#pragma unroll
+  for (int i = 1; i < kNumBins; i++) bin += (b >= a.bin_block[i]);
+  float err = 0.f;
+  switch (bin) {
+    case 0: err = hub_segment<W, DIR, KIND>(a, sredf, ps, pg, pl); break;
+    case 1: err = group_rows<32, W, DIR, KIND>(a, 1, ps, pg, pl); break;
+    case 2: err = group_rows<16, W, DIR, KIND>(a, 2, ps, pg, pl); break;
+    case 3: err = group_rows<8, W, DIR, KIND>(a, 3, ps, pg, pl); break;
+    case 4: err = group_rows<4, W, DIR, KIND>(a, 4, ps, pg, pl); break;
+    case 5: err = group_rows<2, W, DIR, KIND>(a, 5, ps, pg, pl); break;
+    case 6: err = group_rows<1, W, DIR, KIND>(a, 6, ps, pg, pl); break;
+    default: err = zero_rows<W, DIR, KIND>(a, ps, pl); break;
+  }
+  const double block_err = block_sum_d<kSweepThreads>(static_cast<double>(err), sred);
+  grid_finish(a, block_err, sred);
+}
+
+// ---- generic warp-per-row sweep (unsorted CSR, grid-stride) ----------------
+
+template <bool W, int KIND>
+__global__ void __launch_bounds__(kSweepThreads)
+pull_generic_kernel(const PullArgs a) {
+  if (*reinterpret_cast<volatile const int *>(&a.ctl->done)) return;
+  __shared__ double sred[kSweepThreads / 32];
+  const uint64_t ps = policy_evict_first();
+  const uint64_t pg = policy_evict_last();
+  const int lane = threadIdx.x & 31;
+  const int warps = a.nblocks * (kSweepThreads / 32);
+  float err = 0.f;
+  for (int u = blockIdx.x * (kSweepThreads / 32) + (threadIdx.x >> 5); u < a.n; u += warps) {
+    const int s = a.rowoff[u], e = a.rowoff[u + 1];
+    float acc = lane_partial<32, W>(a, s, e, lane, ps, pg);
+    acc = group_sum<32>(acc);
+    if (lane == 0) err += finish_row<W, false, KIND>(a, u, s, e, acc, ps, pg);
+  }
+  const double block_err = block_sum_d<kSweepThreads>(static_cast<double>(err), sred);
+  grid_finish(a, block_err, sred);
+}
+
+cudaError_t LaunchPullGeneric(const PullArgs &a, cudaStream_t s) {
+  if (a.nblocks == 0) return cudaSuccess;
+  const bool W = a.win != nullptr;
+  if (a.kind == kKindAdjoint) {
+    if (W) pull_generic_kernel<true, kKindAdjoint><<<a.nblocks, kSweepThreads, 0, s>>>(a);
+    else pull_generic_kernel<false, kKindAdjoint><<<a.nblocks, kSweepThreads, 0, s>>>(a);
+  } else {
+    if (W) pull_generic_kernel<true, kKindPPR><<<a.nblocks, kSweepThreads, 0, s>>>(a);
+    else pull_generic_kernel<false, kKindPPR><<<a.nblocks, kSweepThreads, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+// ---- adjoint gradients ---------------------------------------------------------
+
+// One warp per renumbered out-row v:
+//   (P lambda)[v] = sum_e w_e lambda[u_e] / S_v
+//   grad_ew[orig position of e] = d s[v] / S_v (lambda[u_e] - (P lambda)[v])
+__global__ void adjoint_edge_grad_kernel(int32_t n, const int32_t *__restrict__ orow,
+                                         const int32_t *__restrict__ ocol,
+                                         const float *__restrict__ wout,
+                                         const float *__restrict__ rsum,
+                                         const int32_t *__restrict__ perm,
+                                         const int32_t *__restrict__ orig_off,
+                                         const float *__restrict__ lam,
+                                         const float *__restrict__ sv, float damping,
+                                         float *grad_ew) {
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int v = static_cast<int>(warp);
+  const int s = orow[v], e = orow[v + 1];
+  if (s == e) return;
+  double acc = 0;
+  for (int j = s + lane; j < e; j += 32)
+    acc += static_cast<double>(wout ? wout[j] : 1.f) * lam[ocol[j]];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  const double S = rsum ? static_cast<double>(rsum[v]) : static_cast<double>(e - s);
+  const double plam = acc / S;
+  const double coef = static_cast<double>(damping) * sv[v] / S;
+  const int64_t base = orig_off[perm[v]];
+  for (int j = s + lane; j < e; j += 32)
+    grad_ew[base + (j - s)] = static_cast<float>(coef * (lam[ocol[j]] - plam));
+}
+
+__global__ void adjoint_teleport_grad_kernel(int32_t n, const int32_t *__restrict__ inv,
+                                             const float *__restrict__ lam, float omd,
+                                             float *grad_t) {
+  const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  grad_t[v] = __fmul_rn(omd, lam[inv[v]]);
+}
+
+cudaError_t LaunchAdjointGrads(const DeviceGraph &g, const int32_t *orow, const int32_t *ocol,
+                               const float *wout, const float *lam_new, const float *s_new,
+                               float damping, float *grad_ew, float *grad_t_old,
+                               cudaStream_t s) {
+  const int n = static_cast<int>(g.n);
+  if (grad_ew) {
+    adjoint_edge_grad_kernel<<<static_cast<unsigned>((static_cast<int64_t>(n) * 32 + 255) / 256), 256, 0, s>>>(
+        n, orow, ocol, wout, g.weighted ? g.rsum : nullptr, g.perm, g.orig_out_off, lam_new, s_new,
+        damping, grad_ew);
+  }
+  if (grad_t_old)
+    adjoint_teleport_grad_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, g.inv, lam_new, 1.0f - damping,
+                                                                 grad_t_old);
+  return cudaGetLastError();
+}
+
+// Deterministic sum_i |x_i| in double: one block, fixed stride order.
+__global__ void l1_norm_kernel(const float *__restrict__ x, int64_t n, double *out) {
+  __shared__ double sred[32];
+  double v = 0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) v += fabs(static_cast<double>(x[i]));
+  const double t = block_sum_d<1024>(v, sred);
+  if (threadIdx.x == 0) *out = t;
+}
+
+cudaError_t LaunchL1Norm(const float *x, int64_t n, double *out, cudaStream_t s) {
+  l1_norm_kernel<<<1, 1024, 0, s>>>(x, n, out);
+  return cudaGetLastError();
+}
+
+// ---- init / permutation kernels ---------------------------------------------
+
+template <bool W, bool DIR>
+__global__ void pull_init_kernel(int32_t n, const int32_t *__restrict__ rowoff,
+                                 const int32_t *__restrict__ odeg,
+                                 const float *__restrict__ rsum,
+                                 const float *__restrict__ tele_new, float init_scalar,
+                                 float one_minus_d, float *score, float *contrib,
+                                 float *base) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  const float t = tele_new ? tele_new[u] : init_scalar;
+  score[u] = t;
+  if (tele_new) base[u] = __fmul_rn(one_minus_d, t);
+  float denom;
+  if (W) denom = rsum[u];
+  else if (DIR) denom = __int2float_rn(odeg[u]);
+  else denom = __int2float_rn(rowoff[u + 1] - rowoff[u]);
+  contrib[u] = __fdiv_rn(t, denom);
+}
+
+__global__ void gather_out_kernel(int32_t n, int ncols, const int32_t *__restrict__ inv,
+                                  const float *__restrict__ src_new, float *dst_old) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<int64_t>(n) * ncols) return;
+  const int64_t v = i / ncols;
+  const int c = static_cast<int>(i - v * ncols);
+  dst_old[i] = src_new[static_cast<int64_t>(inv[v]) * ncols + c];
+}
+
+__global__ void gather_in_kernel(int32_t n, int ncols, const int32_t *__restrict__ perm,
+                                 const float *__restrict__ src_old, float *dst_new) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<int64_t>(n) * ncols) return;
+  const int64_t u = i / ncols;
+  const int c = static_cast<int>(i - u * ncols);
+  dst_new[i] = src_old[static_cast<int64_t>(perm[u]) * ncols + c];
+}
+
+// ---- launchers ---------------------------------------------------------------
+
+int PullBlocks(const DeviceGraph &g, int32_t bin_block[kNumBins + 1]) {
+  int64_t blocks = 0;
+  for (int b = 0; b < kNumBins; b++) {
+    bin_block[b] = static_cast<int32_t>(blocks);
+    const int64_t rows = g.bin_row_start[b + 1] - g.bin_row_start[b];
+    if (b == kBinHub) {
+      blocks += g.num_segments;
+    } else if (b == kBinZero) {
+      const int64_t per = kSweepThreads * kZeroRowsPerThread;
+      blocks += (rows + per - 1) / per;
+    } else {
+      const int64_t per = kSweepThreads / kBinGroup[b];
+      blocks += (rows + per - 1) / per;
+    }
+  }
+  bin_block[kNumBins] = static_cast<int32_t>(blocks);
+  return static_cast<int>(blocks);
+}
+
+cudaError_t LaunchPullSweep(const PullArgs &a, cudaStream_t s) {
+  if (a.nblocks == 0) return cudaSuccess;
+  const bool W = a.win != nullptr, DIR = a.odeg != nullptr;
+  const int kind = a.kind;
+  dim3 grid(a.nblocks), block(kSweepThreads);
+#define PR_LAUNCH(w, d, k) pull_sweep_kernel<w, d, k><<<grid, block, 0, s>>>(a)
+#define PR_KINDS(w, d)                                        \
+  do {                                                        \
+    if (kind == kKindPlain) PR_LAUNCH(w, d, kKindPlain);      \
+    else if (kind == kKindPPR) PR_LAUNCH(w, d, kKindPPR);     \
+    else PR_LAUNCH(w, d, kKindAdjoint);                       \
+  } while (0)
+  if (W) PR_KINDS(true, false);
+  else if (DIR) PR_KINDS(false, true);
+  else PR_KINDS(false, false);
+#undef PR_KINDS
+#undef PR_LAUNCH
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchPullInit(const DeviceGraph &g, Scratch &sc, const float *tele_new,
+                           float init_scalar, float damping, cudaStream_t s) {
+  const int n = static_cast<int>(g.n);
+  if (n == 0) return cudaSuccess;
+  const int threads = 256;
+  const int blocks = (n + threads - 1) / threads;
+  const float omd = 1.0f - damping;
+  if (g.weighted)
+    pull_init_kernel<true, false><<<blocks, threads, 0, s>>>(
+        n, g.rowoff, g.odeg, g.rsum, tele_new, init_scalar, omd, sc.score, sc.contrib[0], sc.base);
+  else if (g.directed)
+    pull_init_kernel<false, true><<<blocks, threads, 0, s>>>(
+        n, g.rowoff, g.odeg, g.rsum, tele_new, init_scalar, omd, sc.score, sc.contrib[0], sc.base);
+  else
+    pull_init_kernel<false, false><<<blocks, threads, 0, s>>>(
+        n, g.rowoff, g.odeg, g.rsum, tele_new, init_scalar, omd, sc.score, sc.contrib[0], sc.base);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchGatherOut(const DeviceGraph &g, const float *src_new, float *dst_old,
+                            int ncols, cudaStream_t s) {
+  const int64_t total = g.n * ncols;
+  if (total == 0) return cudaSuccess;
+  const int threads = 256;
+  const int64_t blocks = (total + threads - 1) / threads;
+  gather_out_kernel<<<static_cast<unsigned>(blocks), threads, 0, s>>>(
+      static_cast<int32_t>(g.n), ncols, g.inv, src_new, dst_old);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchScatterIn(const DeviceGraph &g, const float *src_old, float *dst_new,
+                            int ncols, cudaStream_t s) {
+  const int64_t total = g.n * ncols;
+  if (total == 0) return cudaSuccess;
+  const int threads = 256;
+  const int64_t blocks = (total + threads - 1) / threads;
+  gather_in_kernel<<<static_cast<unsigned>(blocks), threads, 0, s>>>(
+      static_cast<int32_t>(g.n), ncols, g.perm, src_old, dst_new);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchResetCtl(Scratch &sc, int nblocks, int iters, cudaStream_t s) {
+  const int ngroups = (nblocks + kReduceGroup - 1) / kReduceGroup;
+  cudaError_t e = cudaMemsetAsync(sc.ctl, 0, sizeof(SweepCtl), s);
+  if (e != cudaSuccess) return e;
+  if (ngroups) e = cudaMemsetAsync(sc.tick1, 0, sizeof(unsigned) * ngroups, s);
+  if (e != cudaSuccess) return e;
+  if (iters) e = cudaMemsetAsync(sc.trace, 0, sizeof(double) * iters, s);
+  return e;
+}
+
+}  // namespace prgpu

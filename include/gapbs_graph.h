@@ -1,0 +1,73 @@
+/*
+ * gapbs_graph.h -- C ABI of the host graph builder (libgapbs_graph.so).
+ *
+ * Replaces, for callers that are not C++ (the Python package, ctypes, any
+ * FFI), the reference's graph construction entry point
+ * BuilderBase::MakeGraph (src/builder.h:343-364) and the CSRGraph accessors
+ * the PageRank kernel touches (src/graph.h:189-221, VertexOffsets :251-259).
+ * The graph built for a given argument string is identical, offset for offset
+ * and neighbour for neighbour, to the one the reference builds for the same
+ * command line.
+ *
+ * All functions return 0 on success or a negative code (the reference's exit
+ * code for the same condition where it has one); the message is available
+ * from gapbs_graph_last_error() on the calling thread.
+ */
+#ifndef GAPBS_GRAPH_H_
+#define GAPBS_GRAPH_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gapbs_graph gapbs_graph_t;
+
+/* Builds from pr_spmv-style options, e.g. "-g 16", "-u 24 -k 16",
+ * "-f graph.el -s", "-f graph.sg" (src/command_line.h:28-94 option
+ * semantics: -g/-u force symmetrisation).  verbose != 0 prints the
+ * reference's "Generate Time:" / "Read Time:" / "Build Time:" lines. */
+int gapbs_graph_build(gapbs_graph_t **out, const char *args, int verbose);
+
+/* Builds from an explicit edge list u[i] -> v[i] (N = max id + 1, rows
+ * sorted, de-duplicated, self-loops removed; symmetrize != 0 adds reverse
+ * edges).  Mirrors BuilderBase::MakeGraphFromEL + SquishGraph
+ * (src/builder.h:317-341,172-186). */
+int gapbs_graph_from_edges(gapbs_graph_t **out, const int32_t *u,
+                           const int32_t *v, int64_t m, int symmetrize);
+
+/* Writes the .sg serialized layout (src/writer.h:39-69). */
+int gapbs_graph_write_sg(const gapbs_graph_t *g, const char *path);
+
+void gapbs_graph_free(gapbs_graph_t *g);
+
+int64_t gapbs_graph_num_nodes(const gapbs_graph_t *g);
+/* Undirected graphs count each edge once (src/graph.h:193-203). */
+int64_t gapbs_graph_num_edges(const gapbs_graph_t *g);
+int64_t gapbs_graph_num_edges_directed(const gapbs_graph_t *g);
+int gapbs_graph_directed(const gapbs_graph_t *g);
+
+/* CSR views owned by the graph (valid until gapbs_graph_free).  For an
+ * undirected graph the in-views return the out-arrays. */
+const int64_t *gapbs_graph_out_offsets(const gapbs_graph_t *g);
+const int32_t *gapbs_graph_out_neighbors(const gapbs_graph_t *g);
+const int64_t *gapbs_graph_in_offsets(const gapbs_graph_t *g);
+const int32_t *gapbs_graph_in_neighbors(const gapbs_graph_t *g);
+
+/* Prints "Graph has N nodes and M [un]directed edges for degree: D"
+ * (src/graph.h:223-230). */
+void gapbs_graph_print_stats(const gapbs_graph_t *g);
+
+/* The k largest scores as (id, score), in the order and with the tie rule of
+ * the reference's TopK (src/benchmark.h:72-88) as used by PrintTopScores
+ * (src/pr_spmv.cc:64-73).  Returns the number written (<= k). */
+int gapbs_top_scores(const float *scores, int64_t n, int k, int32_t *ids, float *values);
+
+const char *gapbs_graph_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GAPBS_GRAPH_H_ */

@@ -1,0 +1,141 @@
+/*
+ * pr_gpu.h -- C ABI of the B200 PageRank engine (libgapbs_pr.so, sm_100a).
+ *
+ * This is the drop-in boundary for the GAP Benchmark Suite's pull-direction
+ * Jacobi PageRank.  A reference-side caller replaces the body of
+ *
+ *   pvector<ScoreT> PageRankPull(const Graph &g, int max_iters,
+ *                                double epsilon, bool logging_enabled)
+ *                                              (src/pr_spmv.cc:35-61)
+ *
+ * with pr_gpu_upload (once per graph) + pr_gpu_run, and gets the same float
+ * scores (within FP32 summation-order tolerance), the same sweep count and
+ * the same per-sweep L1 error trace (src/pr_spmv.cc:55-58).
+ *
+ * Conventions
+ *   - Every int function returns PR_GPU_OK (0) or a negative PR_GPU_E* code;
+ *     pr_gpu_last_error(h) describes the last failure on that handle.  No
+ *     C++ exception crosses this boundary.
+ *   - All pointers are plain host pointers unless the function name ends in
+ *     _device, in which case they are device pointers on the handle's GPU.
+ *   - Graph ids are int32 (NodeID, src/benchmark.h:31); offsets are int32, so
+ *     an uploaded graph holds at most 2^31-1 CSR entries per direction.
+ *   - Score blocks with ncols columns are vertex-major: element (v, c) lives
+ *     at [v * ncols + c] (an N x ncols row-major block).
+ *   - One handle is used by one host thread at a time.  It owns every device
+ *     allocation; callers own every host buffer they pass.
+ */
+#ifndef GAPBS_PR_GPU_H_
+#define GAPBS_PR_GPU_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PR_GPU_OK 0
+#define PR_GPU_EINVAL (-1)    /* bad argument */
+#define PR_GPU_ECUDA (-2)     /* CUDA runtime error */
+#define PR_GPU_ENOMEM (-3)    /* device or pinned allocation failed */
+#define PR_GPU_ENOGRAPH (-4)  /* no graph uploaded on this handle */
+#define PR_GPU_EGRAPH (-5)    /* CSR failed validation (offsets / ids) */
+#define PR_GPU_ERANGE (-6)    /* graph exceeds int32 offsets */
+
+typedef struct pr_gpu pr_gpu_t;
+
+/* Creates a handle bound to CUDA device `device` with its own stream. */
+int pr_gpu_create(pr_gpu_t **h, int device);
+
+/* Uploads a CSR graph and builds the device mirror (degree-ordered rows and
+ * the vertex bins the sweep uses).  Replaces the CSRGraph the reference's
+ * PageRankPull reads through out_degree / in_neigh (src/graph.h:205-221).
+ *
+ *   n                 number of vertices
+ *   m                 entries per direction (num_edges_directed)
+ *   out_off/out_nbr   out-CSR (n+1 offsets, m neighbour ids)
+ *   in_off/in_nbr     in-CSR; NULL (or equal to out_*) for an undirected
+ *                     graph, whose single CSR serves both directions
+ *                     (src/graph.h:138-143)
+ *   edge_w            optional FP32 weight per out-CSR entry (weight of v->u
+ *                     at v's out-list position); NULL means unit weights.
+ *                     Transition probabilities are w(v->u) / sum_u' w(v->u').
+ *
+ * The CSR is validated on the device (monotone offsets starting at 0 and
+ * ending at m, every id in [0, n)); failures return PR_GPU_EGRAPH.  A new
+ * upload replaces the previous graph. */
+int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m,
+                  const int32_t *out_off, const int32_t *out_nbr,
+                  const int32_t *in_off, const int32_t *in_nbr,
+                  const float *edge_w);
+
+/* Runs Jacobi PageRank sweeps until the L1 change of a sweep is < epsilon or
+ * max_iters sweeps have run (src/pr_spmv.cc:41-58).
+ *
+ *   ncols == 1, teleport == NULL : the reference's PageRankPull exactly
+ *       (init 1/N, base (1-d)/N in float, contrib = score / out_degree).
+ *   teleport != NULL : personalized PageRank, s = (1-d) t + d P^T s started
+ *       from s_0 = t, one column per teleport vector (n x ncols block);
+ *       columns retire independently when their own L1 change < epsilon.
+ *   scores_out   n x ncols floats (caller-owned host buffer)
+ *   sweeps_out   ncols ints: sweeps executed per column (nullable)
+ *   err_trace    max_iters x ncols doubles, [iter * ncols + c], the FP64 L1
+ *                change of each sweep; 0 after a column retired (nullable)
+ * damping is the reference's kDamp (0.85f, src/pr_spmv.cc:33). */
+int pr_gpu_run(pr_gpu_t *h, int max_iters, double epsilon, float damping,
+               int ncols, const float *teleport, float *scores_out,
+               int32_t *sweeps_out, double *err_trace);
+
+/* Same as pr_gpu_run with teleport / scores_out as DEVICE pointers on the
+ * handle's GPU (no host copies; the call still returns after the solve). */
+int pr_gpu_run_device(pr_gpu_t *h, int max_iters, double epsilon,
+                      float damping, int ncols, const float *teleport_dev,
+                      float *scores_out_dev, int32_t *sweeps_out,
+                      double *err_trace);
+
+/* Reverse-mode derivative of L = sum_v loss_w[v] * s[v] at the fixed point
+ * s of the last single-column pr_gpu_run (scores passed back in `scores`).
+ * Solves lambda = w + d P lambda (a gather over OUT-neighbours) until its L1
+ * change < epsilon * ||w||_1 or max_iters sweeps, then
+ *   grad_teleport[u]  = (1-d) lambda[u]
+ *   grad_edge_w[e]    = d s[v] / S_v (lambda[u] - (P lambda)[v]),  e = (v->u)
+ * with grad_edge_w aligned with the uploaded out-CSR (nullable).
+ * The reference has no adjoint; this is the engine's own extension.
+ * Host-pointer form. */
+int pr_gpu_adjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping,
+                   const float *loss_w, const float *scores,
+                   float *grad_teleport, float *grad_edge_w,
+                   int32_t *sweeps_out);
+
+/* Device-pointer form of pr_gpu_adjoint. */
+int pr_gpu_adjoint_device(pr_gpu_t *h, int max_iters, double epsilon,
+                          float damping, const float *loss_w_dev,
+                          const float *scores_dev, float *grad_teleport_dev,
+                          float *grad_edge_w_dev, int32_t *sweeps_out);
+
+/* Makes the handle issue its work on `stream` (a cudaStream_t of the
+ * handle's device, e.g. the caller's framework stream) instead of its own;
+ * NULL restores the handle's own stream.  The handle does not take
+ * ownership.  Calls still synchronize that stream before returning. */
+int pr_gpu_set_stream(pr_gpu_t *h, void *stream);
+
+/* Device time (CUDA events on the handle's stream) of the sweep kernels of
+ * the last run and the number of engine kernel launches it made. */
+int pr_gpu_last_timing(const pr_gpu_t *h, double *sweep_ms, double *total_ms,
+                       int64_t *kernel_launches);
+
+/* Graph facts after upload: vertices, entries, rows per vertex bin
+ * (nbins entries, bin order as documented in the engine), max in-degree. */
+int pr_gpu_graph_info(const pr_gpu_t *h, int64_t *n, int64_t *m,
+                      int64_t *max_degree, int64_t *bin_rows, int nbins);
+
+void pr_gpu_destroy(pr_gpu_t *h);
+
+/* Message for the last failure on h (h may be NULL for create failures). */
+const char *pr_gpu_last_error(const pr_gpu_t *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GAPBS_PR_GPU_H_ */

@@ -1,0 +1,213 @@
+/*
+ * pr_oracle.c -- TEST INFRASTRUCTURE ONLY (the checker, never the product).
+ *
+ * CPU restatement of the reference's pull-direction Jacobi PageRank and of
+ * the PPR / adjoint mathematics the GPU engine implements.  Every function
+ * cites the reference lines it follows.  Compiled with -ffp-contract=off and
+ * without -march so that the FP32 mirror performs exactly the float
+ * operations the reference performs (no fused multiply-add).
+ */
+#include "pr_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+static inline int64_t deg_of(const int64_t *off, int64_t v) {
+  return off[v + 1] - off[v];
+}
+
+/* src/pr_spmv.cc:35-61 */
+int oracle_pr_pull_f32(int64_t n, const int64_t *in_off, const int32_t *in_nbr,
+                       const int64_t *out_off, int max_iters, double epsilon,
+                       float damping, float *scores, double *err_trace) {
+  /* :37-38 -- init and base are computed in float from num_nodes */
+  const float init_score = 1.0f / (float)n;
+  const float base_score = (1.0f - damping) / (float)n;
+  float *contrib = (float *)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+  int sweeps = 0;
+  for (int64_t u = 0; u < n; u++) scores[u] = init_score;        /* :39 */
+  for (int iter = 0; iter < max_iters; iter++) {                    /* :41 */
+    double error = 0;
+    for (int64_t v = 0; v < n; v++)                                 /* :43-45 */
+      contrib[v] = scores[v] / (float)deg_of(out_off, v);
+    for (int64_t u = 0; u < n; u++) {                               /* :46-54 */
+      float incoming_total = 0;
+      for (int64_t e = in_off[u]; e < in_off[u + 1]; e++)
+        incoming_total += contrib[in_nbr[e]];
+      float old_score = scores[u];
+      scores[u] = base_score + damping * incoming_total;
+      error += fabsf(scores[u] - old_score);
+    }
+    if (err_trace) err_trace[iter] = error;
+    sweeps = iter + 1;
+    if (error < epsilon) break;                                     /* :57-58 */
+  }
+  free(contrib);
+  return sweeps;
+}
+
+/* src/pr_spmv.cc:35-61 with double everywhere */
+int oracle_pr_pull_f64(int64_t n, const int64_t *in_off, const int32_t *in_nbr,
+                       const int64_t *out_off, int max_iters, double epsilon,
+                       double damping, double *scores, double *err_trace) {
+  const double init_score = 1.0 / (double)n;
+  const double base_score = (1.0 - damping) / (double)n;
+  double *contrib = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  int sweeps = 0;
+  for (int64_t u = 0; u < n; u++) scores[u] = init_score;
+  for (int iter = 0; iter < max_iters; iter++) {
+    double error = 0;
+    for (int64_t v = 0; v < n; v++) {
+      int64_t d = deg_of(out_off, v);
+      contrib[v] = d ? scores[v] / (double)d : 0.0;
+    }
+    for (int64_t u = 0; u < n; u++) {
+      double incoming_total = 0;
+      for (int64_t e = in_off[u]; e < in_off[u + 1]; e++)
+        incoming_total += contrib[in_nbr[e]];
+      double old_score = scores[u];
+      scores[u] = base_score + damping * incoming_total;
+      error += fabs(scores[u] - old_score);
+    }
+    if (err_trace) err_trace[iter] = error;
+    sweeps = iter + 1;
+    if (error < epsilon) break;
+  }
+  free(contrib);
+  return sweeps;
+}
+
+/* src/pr_spmv.cc:78-94 */
+double oracle_pr_verify_f32(int64_t n, const int64_t *out_off,
+                            const int32_t *out_nbr, float damping,
+                            const float *scores) {
+  const float base_score = (1.0f - damping) / (float)n;
+  float *incoming = (float *)calloc((size_t)(n > 0 ? n : 1), sizeof(float));
+  double error = 0;
+  for (int64_t u = 0; u < n; u++) {                                 /* :82-87 */
+    float outgoing_contrib = scores[u] / (float)deg_of(out_off, u);
+    for (int64_t e = out_off[u]; e < out_off[u + 1]; e++)
+      incoming[out_nbr[e]] += outgoing_contrib;
+  }
+  for (int64_t v = 0; v < n; v++)                                   /* :88-91 */
+    error += fabsf(base_score + damping * incoming[v] - scores[v]);
+  free(incoming);
+  return error;
+}
+
+double oracle_pr_residual_f64(int64_t n, const int64_t *in_off,
+                              const int32_t *in_nbr, const int64_t *out_off,
+                              float damping, const float *scores) {
+  const double base = (double)((1.0f - damping) / (float)n);
+  const double d = (double)damping;
+  double error = 0;
+  #pragma omp parallel for reduction(+ : error) schedule(dynamic, 4096)
+  for (int64_t u = 0; u < n; u++) {
+    double acc = 0;
+    for (int64_t e = in_off[u]; e < in_off[u + 1]; e++) {
+      int32_t v = in_nbr[e];
+      acc += (double)scores[v] / (double)deg_of(out_off, v);
+    }
+    error += fabs(base + d * acc - (double)scores[u]);
+  }
+  return error;
+}
+
+/* Row sums S_v: explicit or out-degree. */
+static inline double rowsum_of(const double *rowsum, const int64_t *out_off,
+                               int64_t v) {
+  return rowsum ? rowsum[v] : (double)deg_of(out_off, v);
+}
+
+int oracle_ppr_f64_from(int64_t n, const int64_t *in_off, const int32_t *in_nbr,
+                        const double *in_w, const double *rowsum,
+                        const int64_t *out_off, double damping, const double *t,
+                        const double *s_init, int max_iters, double epsilon,
+                        double *s, double *err_trace) {
+  double *contrib = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  int sweeps = 0;
+  if (s != s_init) memcpy(s, s_init, sizeof(double) * (size_t)n);
+  for (int iter = 0; iter < max_iters; iter++) {
+    double error = 0;
+    for (int64_t v = 0; v < n; v++) {
+      double sv = rowsum_of(rowsum, out_off, v);
+      contrib[v] = sv != 0.0 ? s[v] / sv : 0.0;
+    }
+    #pragma omp parallel for reduction(+ : error) schedule(dynamic, 4096)
+    for (int64_t u = 0; u < n; u++) {
+      double acc = 0;
+      for (int64_t e = in_off[u]; e < in_off[u + 1]; e++)
+        acc += (in_w ? in_w[e] : 1.0) * contrib[in_nbr[e]];
+      double nv = (1.0 - damping) * t[u] + damping * acc;
+      error += fabs(nv - s[u]);
+      s[u] = nv;
+    }
+    if (err_trace) err_trace[iter] = error;
+    sweeps = iter + 1;
+    if (error < epsilon) break;
+  }
+  free(contrib);
+  return sweeps;
+}
+
+int oracle_ppr_f64(int64_t n, const int64_t *in_off, const int32_t *in_nbr,
+                   const double *in_w, const double *rowsum,
+                   const int64_t *out_off, double damping, const double *t,
+                   int max_iters, double epsilon, double *s, double *err_trace) {
+  return oracle_ppr_f64_from(n, in_off, in_nbr, in_w, rowsum, out_off, damping,
+                             t, t, max_iters, epsilon, s, err_trace);
+}
+
+int oracle_ppr_adjoint_f64(int64_t n, const int64_t *out_off,
+                           const int32_t *out_nbr, const double *out_w,
+                           double damping, const double *loss_w,
+                           const double *s, int max_iters, double epsilon,
+                           double *lambda, double *grad_t, double *grad_ew) {
+  double *next = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  double *plam = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  double wnorm = 0;
+  for (int64_t v = 0; v < n; v++) wnorm += fabs(loss_w[v]);
+  const double tol = epsilon * wnorm;
+  int sweeps = 0;
+  memcpy(lambda, loss_w, sizeof(double) * (size_t)n);
+  for (int iter = 0; iter < max_iters; iter++) {
+    double error = 0;
+    #pragma omp parallel for reduction(+ : error) schedule(dynamic, 4096)
+    for (int64_t v = 0; v < n; v++) {
+      double acc = 0, sv = 0;
+      for (int64_t e = out_off[v]; e < out_off[v + 1]; e++) {
+        double w = out_w ? out_w[e] : 1.0;
+        acc += w * lambda[out_nbr[e]];
+        sv += w;
+      }
+      double pl = sv != 0.0 ? acc / sv : 0.0;
+      next[v] = loss_w[v] + damping * pl;
+      error += fabs(next[v] - lambda[v]);
+    }
+    memcpy(lambda, next, sizeof(double) * (size_t)n);
+    sweeps = iter + 1;
+    if (error < tol) break;
+  }
+  /* P lambda at the final lambda, for the edge-weight gradient */
+  #pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t v = 0; v < n; v++) {
+    double acc = 0, sv = 0;
+    for (int64_t e = out_off[v]; e < out_off[v + 1]; e++) {
+      double w = out_w ? out_w[e] : 1.0;
+      acc += w * lambda[out_nbr[e]];
+      sv += w;
+    }
+    plam[v] = sv != 0.0 ? acc / sv : 0.0;
+    if (grad_ew) {
+      for (int64_t e = out_off[v]; e < out_off[v + 1]; e++)
+        grad_ew[e] = sv != 0.0
+            ? damping * s[v] / sv * (lambda[out_nbr[e]] - plam[v]) : 0.0;
+    }
+  }
+  if (grad_t)
+    for (int64_t u = 0; u < n; u++) grad_t[u] = (1.0 - damping) * lambda[u];
+  free(next);
+  free(plam);
+  return sweeps;
+}

@@ -1,0 +1,173 @@
+"""Regenerates the golden fixtures in this directory from the REFERENCE.
+
+Runs only where the reference tree and oracle/_ref (the reference compiled
+from its own sources by oracle/Makefile) exist.  Writes:
+
+  graphs/4*.{el,wel,gr,graph,mtx}   the reference's tiny loader fixtures
+                                     (test/graphs/), copied as test inputs
+  pr_golden.json                     per case: graph identity (N, edge counts,
+                                     sha256 of the CSR arrays), the reference
+                                     PageRankPull's sweep count, its -l lines,
+                                     sha256 of its float32 scores, top-5, and
+                                     PRVerifier's total error
+  scores_<case>.npy                  the reference's float32 scores (small
+                                     graphs only)
+  adversarial.npz                    small hand-made edge lists (isolated
+                                     vertices, star hub, chain, directed sinks)
+                                     with the reference's scores on each
+
+Usage:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF_TREE = "/root/reference"
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+
+
+def sha(*arrays) -> str:
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def capture_stdout(fn, *args, **kw):
+    """Run fn with the process's fd 1 redirected to a temp file; return (ret, text)."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    with tempfile.TemporaryFile(mode="w+b") as tmp:
+        os.dup2(tmp.fileno(), 1)
+        try:
+            ret = fn(*args, **kw)
+        finally:
+            sys.stdout.flush()
+            os.dup2(saved, 1)
+            os.close(saved)
+        tmp.seek(0)
+        text = tmp.read().decode()
+    return ret, text
+
+
+GRAPH_FILES = ["4.el", "4.wel", "4.gr", "4.graph", "4.mtx", "4w.graph", "4w.mtx"]
+
+# (case name, pr_spmv arguments, keep full score vector)
+CASES = [
+    ("g10", "-g 10", True),
+    ("u10", "-u 10", True),
+    ("g12", "-g 12", True),
+    ("u12", "-u 12", False),
+    ("g10k4", "-g 10 -k 4", True),
+    ("g16", "-g 16", False),
+    ("u16", "-u 16", False),
+    ("g18", "-g 18", False),
+    ("el4", "-f {graphs}/4.el", True),
+    ("el4s", "-f {graphs}/4.el -s", True),
+    ("wel4", "-f {graphs}/4.wel", False),
+    ("gr4", "-f {graphs}/4.gr", False),
+    ("graph4", "-f {graphs}/4.graph", False),
+    ("mtx4", "-f {graphs}/4.mtx", False),
+    ("graph4w", "-f {graphs}/4w.graph", False),
+    ("mtx4w", "-f {graphs}/4w.mtx", False),
+]
+
+
+def adversarial_edge_lists():
+    """Small graphs that exercise the corner cases of the sweep."""
+    cases = {}
+    # isolated vertices interleaved with a triangle and a pendant: ids 0..9
+    cases["isolated"] = (np.array([1, 2, 3, 3, 9], np.int32), np.array([2, 3, 1, 7, 3], np.int32), True)
+    # star: hub 0 with 300 leaves (hub degree above a warp and a block)
+    leaves = np.arange(1, 301, dtype=np.int32)
+    cases["star"] = (np.zeros_like(leaves), leaves, True)
+    # chain of 50
+    a = np.arange(0, 49, dtype=np.int32)
+    cases["chain"] = (a, a + 1, True)
+    # directed with sinks (vertices with no out-edges) and sources
+    u = np.array([0, 0, 1, 2, 2, 3, 5, 5, 6, 7], np.int32)
+    v = np.array([1, 2, 3, 3, 4, 4, 4, 6, 4, 0], np.int32)
+    cases["directed_sinks"] = (u, v, False)
+    # self loops and duplicates only (squish removes them)
+    cases["selfdup"] = (np.array([0, 0, 1, 1, 2, 2, 2], np.int32), np.array([0, 1, 0, 1, 2, 0, 0], np.int32), True)
+    # one big hub (degree 5000) plus a random sparse remainder
+    rng = np.random.default_rng(7)
+    hu = np.zeros(5000, np.int32)
+    hv = rng.integers(1, 6000, 5000).astype(np.int32)
+    ru = rng.integers(1, 6000, 20000).astype(np.int32)
+    rv = rng.integers(1, 6000, 20000).astype(np.int32)
+    cases["hub5000"] = (np.concatenate([hu, ru]), np.concatenate([hv, rv]), True)
+    return cases
+
+
+def main():
+    if not os.path.isdir(REF_TREE) or not oracle.ref_available():
+        sys.exit("needs the reference tree and oracle/_ref (make -C oracle)")
+    gdir = os.path.join(HERE, "graphs")
+    os.makedirs(gdir, exist_ok=True)
+    for f in GRAPH_FILES:
+        shutil.copyfile(os.path.join(REF_TREE, "test", "graphs", f), os.path.join(gdir, f))
+    expected = {}
+    for f in os.listdir(os.path.join(REF_TREE, "test", "reference")):
+        with open(os.path.join(REF_TREE, "test", "reference", f)) as fh:
+            expected[f] = fh.read().strip()
+
+    out = {"generator": "tests/golden/make_golden.py", "reference_outputs": expected, "cases": {}}
+    for name, args, keep in CASES:
+        a = args.format(graphs=gdir)
+        g, _ = capture_stdout(oracle.RefGraph.build, a)
+        oo, onb, io, inb = g.csr()
+        scores, log = capture_stdout(g.pagerank_pull, 20, 1e-4, True)
+        step_lines = [ln for ln in log.splitlines() if ln.strip()]
+        ok, vlog = capture_stdout(g.verify, scores, 1e-4)
+        order = np.lexsort((np.arange(scores.size), -scores.astype(np.float64)))[:5]
+        entry = {
+            "args": args,
+            "num_nodes": g.num_nodes,
+            "num_edges": g.num_edges,
+            "num_edges_directed": g.num_edges_directed,
+            "directed": g.directed,
+            "csr_sha256": sha(oo, onb, io, inb),
+            "sweeps": len(step_lines),
+            "log_lines": step_lines,
+            "scores_sha256": sha(scores),
+            "scores_sum": float(scores.astype(np.float64).sum()),
+            "top5": [[int(i), float(scores[i])] for i in order],
+            "verify_pass": ok,
+            "verify_line": vlog.strip(),
+        }
+        if keep:
+            np.save(os.path.join(HERE, f"scores_{name}.npy"), scores)
+        out["cases"][name] = entry
+        print(name, g.num_nodes, g.num_edges, entry["sweeps"], ok)
+
+    adv = {}
+    for name, (u, v, sym) in adversarial_edge_lists().items():
+        from gapbs_b200.graph import Graph
+        hg = Graph.from_edges(u, v, symmetrize=sym)
+        rg = oracle.RefGraph.from_csr(hg)
+        scores, log = capture_stdout(rg.pagerank_pull, 20, 1e-4, True)
+        adv[f"{name}_u"] = u
+        adv[f"{name}_v"] = v
+        adv[f"{name}_sym"] = np.array(sym)
+        adv[f"{name}_scores"] = scores
+        adv[f"{name}_sweeps"] = np.array(len([ln for ln in log.splitlines() if ln.strip()]))
+        print("adversarial", name, hg.num_nodes, hg.num_edges_directed)
+    np.savez_compressed(os.path.join(HERE, "adversarial.npz"), **adv)
+    with open(os.path.join(HERE, "pr_golden.json"), "w") as fh:
+        json.dump(out, fh, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,157 @@
+"""GPU parity of the plain PageRankPull path (through the C ABI).
+
+Checked against the oracle (the FP32 mirror reproduces the reference bit for
+bit; the FP64 restatement is the accuracy yardstick) on the reference's own
+graphs and on hand-made corner cases.
+
+Tolerances (FP32 scores summed in a different order than the reference):
+  * sweep count identical to the reference's;
+  * L1(gpu - fp64) <= 4 * L1(reference_fp32 - fp64) + 1e-7;
+  * |gpu - fp64| <= 2e-5 * |fp64| + 1e-10 per vertex;
+  * PRVerifier total error < epsilon (the reference's pass criterion);
+  * per-sweep L1 errors within 1e-3 relative + 1e-6 of the reference's.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from gapbs_b200 import PageRankEngine, PageRankPull
+from gapbs_b200.graph import Graph, make_graph
+from conftest import golden_args, gpu_available, fmt_step
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["g10", "u10", "g12", "u12", "g10k4", "g16", "u16", "g18", "el4", "el4s", "mtx4"]
+
+
+@pytest.fixture(scope="module")
+def engine():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    eng = PageRankEngine(0)
+    yield eng
+    eng.close()
+
+
+def check_parity(engine, g, max_iters=20, epsilon=1e-4, expect_sweeps=None):
+    engine.upload(g)
+    res = engine.run(max_iters, epsilon)
+    s32, k32, tr32 = oracle.pr_pull_f32(g, max_iters, epsilon)
+    s64, _, _ = oracle.pr_pull_f64(g, max_iters, epsilon)
+    gpu = res.scores
+    assert gpu.dtype == np.float32 and gpu.shape == (g.num_nodes,)
+    assert int(res.sweeps[0]) == k32
+    if expect_sweeps is not None:
+        assert k32 == expect_sweeps
+    ref_l1 = float(np.abs(s32.astype(np.float64) - s64).sum())
+    gpu_l1 = float(np.abs(gpu.astype(np.float64) - s64).sum())
+    assert gpu_l1 <= 4 * ref_l1 + 1e-7, (gpu_l1, ref_l1)
+    assert np.all(np.abs(gpu - s64) <= 2e-5 * np.abs(s64) + 1e-10)
+    if epsilon > 0 and k32 < max_iters:
+        assert oracle.pr_verify_f32(g, gpu) < epsilon
+    np.testing.assert_allclose(res.err_trace[:k32, 0], tr32, rtol=1e-3, atol=1e-6)
+    return res
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_parity_reference_graphs(engine, golden, case):
+    e = golden["cases"][case]
+    g = make_graph(golden_args(e))
+    check_parity(engine, g, expect_sweeps=e["sweeps"])
+
+
+def test_parity_adversarial(engine, adversarial):
+    names = sorted({k.rsplit("_", 1)[0] for k in adversarial if k.endswith("_scores")})
+    for name in names:
+        g = Graph.from_edges(adversarial[f"{name}_u"], adversarial[f"{name}_v"],
+                             symmetrize=bool(adversarial[f"{name}_sym"]))
+        check_parity(engine, g, expect_sweeps=int(adversarial[f"{name}_sweeps"]))
+
+
+def test_multi_segment_hubs(engine):
+    """Rows longer than one hub segment (8192 entries) in several sizes."""
+    rng = np.random.default_rng(11)
+    us, vs = [], []
+    for hub, deg in ((0, 30000), (1, 8192), (2, 8193), (3, 16385)):
+        us.append(np.full(deg, hub))
+        vs.append(rng.integers(10, 40000, deg))
+    us.append(rng.integers(10, 40000, 60000))
+    vs.append(rng.integers(10, 40000, 60000))
+    g = Graph.from_edges(np.concatenate(us), np.concatenate(vs), symmetrize=True)
+    check_parity(engine, g)
+
+
+def test_directed_with_sinks_and_sources(engine):
+    rng = np.random.default_rng(5)
+    u = rng.integers(0, 3000, 20000)
+    v = rng.integers(0, 3000, 20000)
+    v[:500] = 7          # a hub sink
+    u[500:1500] = 9      # a hub source
+    g = Graph.from_edges(u, v, symmetrize=False)
+    assert g.directed
+    check_parity(engine, g)
+
+
+def test_zero_iterations_returns_init(engine):
+    g = make_graph("-g 10")
+    engine.upload(g)
+    res = engine.run(0, 1e-4)
+    assert int(res.sweeps[0]) == 0
+    assert np.all(res.scores == np.float32(1.0) / np.float32(g.num_nodes))
+
+
+def test_epsilon_zero_runs_all_iterations(engine):
+    g = make_graph("-u 10")
+    res = check_parity(engine, g, max_iters=20, epsilon=0.0)
+    assert int(res.sweeps[0]) == 20
+
+
+def test_deterministic(engine):
+    g = make_graph("-g 14")
+    engine.upload(g)
+    a = engine.run(20, 1e-4)
+    b = engine.run(20, 1e-4)
+    assert np.array_equal(a.scores.view(np.uint32), b.scores.view(np.uint32))
+    assert np.array_equal(a.err_trace, b.err_trace)
+
+
+def test_pagerankpull_logging(engine, golden, capfd):
+    e = golden["cases"]["g12"]
+    g = make_graph(golden_args(e))
+    s = PageRankPull(g, 20, 1e-4, logging_enabled=True)
+    out = capfd.readouterr().out.strip().splitlines()
+    assert len(out) == e["sweeps"]
+    # same step numbers; values agree to the printed precision or one unit
+    for got, want in zip(out, e["log_lines"]):
+        assert got[:5] == want[:5]
+        assert abs(float(got[5:]) - float(want[5:])) <= 1.01e-5
+    assert s.dtype == np.float32
+
+
+def test_invalid_csr_rejected(engine):
+    from gapbs_b200.pagerank import PageRankError
+    with pytest.raises(PageRankError) as ei:
+        engine.upload_csr(3, [0, 1, 2, 3], [1, 2, 5])   # id 5 out of range
+    assert ei.value.code == -5
+    with pytest.raises(PageRankError) as ei:
+        engine.upload_csr(3, [0, 2, 1, 3], [1, 2, 0])   # offsets not monotone
+    assert ei.value.code == -5
+
+
+def test_run_without_graph_fails_cleanly():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from gapbs_b200.pagerank import PageRankError
+    eng = PageRankEngine(0)
+    with pytest.raises(PageRankError) as ei:
+        eng.run(20, 1e-4)
+    assert ei.value.code == -4
+    eng.close()
+
+
+def test_bins_cover_all_rows(engine):
+    g = make_graph("-g 16")
+    engine.upload(g)
+    info = engine.graph_info()
+    assert sum(info["bin_rows"]) == g.num_nodes
+    assert info["max_degree"] == int(np.diff(g.in_offsets).max())
