@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "batched.h"
@@ -39,8 +40,8 @@ struct BatchArgs {
   const float *__restrict__ base;
   float damping;
   float *S;
-  const float *__restrict__ Cin;
-  float *Cout;
+  float *C0;   // contrib ping-pong: sweep k gathers C[k & 1], writes C[(k + 1) & 1]
+  float *C1;
   int32_t nseg;
   int32_t hub_rows;
   int32_t zero_start;
@@ -56,7 +57,6 @@ struct BatchArgs {
   double *trace;
   int32_t *sweeps;
   int32_t nblocks;
-  int32_t iter;
   double epsilon;
 };
 
@@ -70,9 +70,9 @@ __device__ __forceinline__ float bdenom(const BatchArgs &a, int u) {
 // Warp accumulates sum over entries [s, e) of w_e * Cin[v_e, c] for its two
 // columns; indices are loaded 32 at a time and broadcast by shuffle.
 template <bool W>
-__device__ __forceinline__ void warp_accumulate(const BatchArgs &a, int s, int e, int lane,
-                                                bool a0, bool a1, float &acc0, float &acc1,
-                                                uint64_t ps, uint64_t pg) {
+__device__ __forceinline__ void warp_accumulate(const BatchArgs &a, const float *Cin, int s, int e,
+                                                int lane, bool a0, bool a1, float &acc0,
+                                                float &acc1, uint64_t ps, uint64_t pg) {
   const int B = a.B;
   for (int j0 = s; j0 < e; j0 += 32) {
     const int j = j0 + lane;
@@ -97,10 +97,10 @@ __device__ __forceinline__ void warp_accumulate(const BatchArgs &a, int s, int e
         w3 = __shfl_sync(0xffffffffu, w, k + 3);
       }
       if (a0) {
-        const float x0 = ld_gather(a.Cin + static_cast<int64_t>(v0) * B + lane, pg);
-        const float x1 = ld_gather(a.Cin + static_cast<int64_t>(v1) * B + lane, pg);
-        const float x2 = ld_gather(a.Cin + static_cast<int64_t>(v2) * B + lane, pg);
-        const float x3 = ld_gather(a.Cin + static_cast<int64_t>(v3) * B + lane, pg);
+        const float x0 = ld_gather(Cin + static_cast<int64_t>(v0) * B + lane, pg);
+        const float x1 = ld_gather(Cin + static_cast<int64_t>(v1) * B + lane, pg);
+        const float x2 = ld_gather(Cin + static_cast<int64_t>(v2) * B + lane, pg);
+        const float x3 = ld_gather(Cin + static_cast<int64_t>(v3) * B + lane, pg);
         if (W) {
           acc0 = __fmaf_rn(w0, x0, acc0); acc0 = __fmaf_rn(w1, x1, acc0);
           acc0 = __fmaf_rn(w2, x2, acc0); acc0 = __fmaf_rn(w3, x3, acc0);
@@ -109,10 +109,10 @@ __device__ __forceinline__ void warp_accumulate(const BatchArgs &a, int s, int e
         }
       }
       if (a1) {
-        const float x0 = ld_gather(a.Cin + static_cast<int64_t>(v0) * B + 32 + lane, pg);
-        const float x1 = ld_gather(a.Cin + static_cast<int64_t>(v1) * B + 32 + lane, pg);
-        const float x2 = ld_gather(a.Cin + static_cast<int64_t>(v2) * B + 32 + lane, pg);
-        const float x3 = ld_gather(a.Cin + static_cast<int64_t>(v3) * B + 32 + lane, pg);
+        const float x0 = ld_gather(Cin + static_cast<int64_t>(v0) * B + 32 + lane, pg);
+        const float x1 = ld_gather(Cin + static_cast<int64_t>(v1) * B + 32 + lane, pg);
+        const float x2 = ld_gather(Cin + static_cast<int64_t>(v2) * B + 32 + lane, pg);
+        const float x3 = ld_gather(Cin + static_cast<int64_t>(v3) * B + 32 + lane, pg);
         if (W) {
           acc1 = __fmaf_rn(w0, x0, acc1); acc1 = __fmaf_rn(w1, x1, acc1);
           acc1 = __fmaf_rn(w2, x2, acc1); acc1 = __fmaf_rn(w3, x3, acc1);
@@ -125,11 +125,11 @@ __device__ __forceinline__ void warp_accumulate(const BatchArgs &a, int s, int e
       const int v = __shfl_sync(0xffffffffu, idx, k);
       const float wk = W ? __shfl_sync(0xffffffffu, w, k) : 1.f;
       if (a0) {
-        const float x = ld_gather(a.Cin + static_cast<int64_t>(v) * B + lane, pg);
+        const float x = ld_gather(Cin + static_cast<int64_t>(v) * B + lane, pg);
         acc0 = W ? __fmaf_rn(wk, x, acc0) : acc0 + x;
       }
       if (a1) {
-        const float x = ld_gather(a.Cin + static_cast<int64_t>(v) * B + 32 + lane, pg);
+        const float x = ld_gather(Cin + static_cast<int64_t>(v) * B + 32 + lane, pg);
         acc1 = W ? __fmaf_rn(wk, x, acc1) : acc1 + x;
       }
     }
@@ -138,19 +138,22 @@ __device__ __forceinline__ void warp_accumulate(const BatchArgs &a, int s, int e
 
 // Updates column c of row u; returns |new - old|.
 template <bool W, bool DIR>
-__device__ __forceinline__ double bfinish(const BatchArgs &a, int u, int c, float sum,
+__device__ __forceinline__ double bfinish(const BatchArgs &a, float *Cout, int u, int c, float sum,
                                           float denom, uint64_t ps, uint64_t pl) {
   const int64_t i = static_cast<int64_t>(u) * a.B + c;
   const float old = ld_score(a.S + i, ps);
   const float nw = __fadd_rn(a.base[i], __fmul_rn(a.damping, sum));
   st_hint_f32(a.S + i, nw, ps);
-  st_hint_f32(a.Cout + i, __fdiv_rn(nw, denom), pl);
+  st_hint_f32(Cout + i, __fdiv_rn(nw, denom), pl);
   return static_cast<double>(fabsf(__fsub_rn(nw, old)));
 }
 
 template <bool W, bool DIR>
 __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
-  if (*reinterpret_cast<volatile const int *>(&a.ctl->done)) return;
+  if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
+  const int it = *reinterpret_cast<volatile const int *>(&a.ctl->loop.loops);
+  const float *Cin = (it & 1) ? a.C1 : a.C0;
+  float *Cout = (it & 1) ? a.C0 : a.C1;
   __shared__ double serr[kBW][kMaxTile];
   __shared__ float sacc[kBW][kMaxTile];
   __shared__ int s_last;
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
     const int per = (e - s + kBW - 1) / kBW;
     const int ws = min(e, s + wid * per), we = min(e, ws + per);
     float acc0 = 0.f, acc1 = 0.f;
-    warp_accumulate<W>(a, ws, we, lane, a0, a1, acc0, acc1, ps, pg);
+    warp_accumulate<W>(a, Cin, ws, we, lane, a0, a1, acc0, acc1, ps, pg);
     sacc[wid][lane] = acc0;
     sacc[wid][lane + 32] = acc1;
     __syncthreads();
@@ -198,7 +201,7 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
         float sum = 0.f;
         for (int k = 0; k < nseg; k++)
           sum = __fadd_rn(sum, __ldcg(a.seg_partial + static_cast<int64_t>(first + k) * a.B + c));
-        dcol = bfinish<W, DIR>(a, u, c, sum, bdenom<W, DIR>(a, u), ps, pg);
+        dcol = bfinish<W, DIR>(a, Cout, u, c, sum, bdenom<W, DIR>(a, u), ps, pg);
       }
       if (threadIdx.x == 0) a.hub_ticket[u] = 0;
     }
@@ -213,10 +216,10 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
     for (int u = a.hub_rows + gw; u < a.n; u += W_all) {
       float acc0 = 0.f, acc1 = 0.f;
       if (u < a.zero_start)
-        warp_accumulate<W>(a, a.rowoff[u], a.rowoff[u + 1], lane, a0, a1, acc0, acc1, ps, pg);
+        warp_accumulate<W>(a, Cin, a.rowoff[u], a.rowoff[u + 1], lane, a0, a1, acc0, acc1, ps, pg);
       const float den = bdenom<W, DIR>(a, u);
-      if (a0) e0 += bfinish<W, DIR>(a, u, lane, acc0, den, ps, pg);
-      if (a1) e1 += bfinish<W, DIR>(a, u, lane + 32, acc1, den, ps, pg);
+      if (a0) e0 += bfinish<W, DIR>(a, Cout, u, lane, acc0, den, ps, pg);
+      if (a1) e1 += bfinish<W, DIR>(a, Cout, u, lane + 32, acc1, den, ps, pg);
     }
     serr[wid][lane] = e0;
     serr[wid][lane + 32] = e1;
@@ -264,8 +267,8 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
   if (threadIdx.x < B && ((active >> threadIdx.x) & 1ull)) {
     double tot = 0;
     for (int i = 0; i < ngroups; i++) tot += __ldcg(a.part2 + static_cast<int64_t>(i) * B + threadIdx.x);
-    a.trace[static_cast<int64_t>(a.iter) * B + threadIdx.x] = tot;
-    a.sweeps[threadIdx.x] = a.iter + 1;
+    a.trace[static_cast<int64_t>(it) * B + threadIdx.x] = tot;
+    a.sweeps[threadIdx.x] = it + 1;
     if (tot < a.epsilon) atomicOr(&s_retire, 1ull << threadIdx.x);
   }
   __syncthreads();
@@ -273,7 +276,7 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
     const unsigned long long next = active & ~s_retire;
     a.ctl->active = next;
     a.ctl->tick2 = 0;
-    if (next == 0ull) a.ctl->done = 1;
+    if (next == 0ull) a.ctl->loop.done = 1;
     __threadfence();
   }
 }
@@ -320,13 +323,24 @@ cudaError_t GrowB(T **p, int64_t *cap, int64_t need) {
 }  // namespace
 
 void FreeBatchScratch(BatchScratch *b) {
-  void *ptrs[] = {b->S, b->C[0], b->C[1], b->base, b->part1, b->part2, b->trace,
-                  b->tick1, b->sweeps, b->seg_partial, b->ctl};
-  for (void *p : ptrs)
-    if (p) cudaFree(p);
-  const int tile = b->tile;
-  *b = BatchScratch();
-  b->tile = tile;
+  b->loop.Reset();
+  float **fp[] = {&b->S, &b->C[0], &b->C[1], &b->base, &b->seg_partial};
+  for (float **p : fp) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  double **dp[] = {&b->part1, &b->part2, &b->trace};
+  for (double **p : dp) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  if (b->tick1) cudaFree(b->tick1);
+  if (b->sweeps) cudaFree(b->sweeps);
+  if (b->ctl) cudaFree(b->ctl);
+  b->tick1 = nullptr;
+  b->sweeps = nullptr;
+  b->ctl = nullptr;
+  b->cap_cells = b->cap_part = b->cap_trace = b->cap_seg = 0;
 }
 
 #define PB_TRY(expr)                                                   \
@@ -403,15 +417,16 @@ cudaError_t SolveBatched(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s,
       batch_init_kernel<false, false><<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, ncols, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base);
     nl++;
     BatchCtl ctl0;
+    std::memset(&ctl0, 0, sizeof(ctl0));
     ctl0.active = (B == 64) ? ~0ull : ((1ull << B) - 1ull);
-    ctl0.done = max_iters == 0 ? 1 : 0;
-    ctl0.tick2 = 0;
+    ctl0.loop.done = max_iters == 0 ? 1 : 0;
     PB_TRY(cudaMemcpyAsync(bs.ctl, &ctl0, sizeof(ctl0), cudaMemcpyHostToDevice, s));
     PB_TRY(cudaMemsetAsync(bs.tick1, 0, sizeof(unsigned) * (ngroups + 1), s));
     PB_TRY(cudaMemsetAsync(bs.sweeps, 0, sizeof(int32_t) * kMaxTile, s));
     if (max_iters)
       PB_TRY(cudaMemsetAsync(bs.trace, 0, sizeof(double) * static_cast<int64_t>(max_iters) * B, s));
     BatchArgs a;
+    std::memset(&a, 0, sizeof(a));
     a.n = static_cast<int32_t>(n);
     a.B = B;
     a.rowoff = g.rowoff;
@@ -438,17 +453,13 @@ cudaError_t SolveBatched(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s,
     a.sweeps = bs.sweeps;
     a.nblocks = nblocks;
     a.epsilon = epsilon;
+    a.C0 = bs.C[0];
+    a.C1 = bs.C[1];
+    const void *fn = g.weighted ? reinterpret_cast<const void *>(batch_sweep_kernel<true, false>)
+                   : g.directed ? reinterpret_cast<const void *>(batch_sweep_kernel<false, true>)
+                                : reinterpret_cast<const void *>(batch_sweep_kernel<false, false>);
     PB_TRY(cudaEventRecord(ev[1], s));
-    for (int it = 0; it < max_iters; it++) {
-      a.iter = it;
-      a.Cin = bs.C[it & 1];
-      a.Cout = bs.C[(it + 1) & 1];
-      if (g.weighted) batch_sweep_kernel<true, false><<<nblocks, kBT, 0, s>>>(a);
-      else if (g.directed) batch_sweep_kernel<false, true><<<nblocks, kBT, 0, s>>>(a);
-      else batch_sweep_kernel<false, false><<<nblocks, kBT, 0, s>>>(a);
-      nl++;
-    }
-    PB_TRY(cudaGetLastError());
+    PB_TRY(bs.loop.Launch(fn, dim3(nblocks), dim3(kBT), &a, sizeof(a), &bs.ctl->loop, max_iters, s));
     PB_TRY(cudaEventRecord(ev[2], s));
     batch_out_kernel<<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, ncols, c0, g.inv, bs.S, out_old);
     nl++;
@@ -461,6 +472,9 @@ cudaError_t SolveBatched(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s,
     float ms = 0;
     cudaEventElapsedTime(&ms, ev[1], ev[2]);
     sweep_total += ms;
+    int tile_loops = 0;
+    for (int c = 0; c < B; c++) tile_loops = std::max(tile_loops, sweeps_tile[c]);
+    nl += 2 * tile_loops;  // sweep + decide kernel per executed sweep
     for (int c = 0; c < B; c++) {
       if (sweeps_out) sweeps_out[c0 + c] = sweeps_tile[c];
       if (err_trace)

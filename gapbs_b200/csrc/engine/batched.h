@@ -15,9 +15,10 @@ namespace prgpu {
 constexpr int kMaxTile = 64;
 
 struct BatchCtl {
+  LoopCtl loop;               // done flag + sweep index (see loop_graph.h)
+  unsigned tick2;             // stage-2 ticket of the grid reduction
+  int pad;
   unsigned long long active;  // bit c set while column c of the tile iterates
-  int done;
-  unsigned tick2;
 };
 
 struct BatchScratch {
@@ -29,6 +30,7 @@ struct BatchScratch {
   BatchCtl *ctl = nullptr;
   int64_t cap_cells = 0, cap_part = 0, cap_trace = 0, cap_seg = 0;
   int tile = 0;  // column tile width (0 = automatic)
+  LoopGraph loop;
 };
 
 void FreeBatchScratch(BatchScratch *b);

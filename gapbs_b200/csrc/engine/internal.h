@@ -17,6 +17,8 @@
 #include <string>
 #include <vector>
 
+#include "loop_graph.h"
+
 namespace prgpu {
 
 // Vertex bins, in row order (rows sorted by descending length):
@@ -72,12 +74,11 @@ struct DeviceGraph {
   float *seg_partial = nullptr;   // per segment
 };
 
-// Per-sweep convergence control, in device memory.
+// Per-solve convergence control, in device memory.
 struct SweepCtl {
-  int done;
-  int sweeps;
-  unsigned tick2;
-  int pad;
+  LoopCtl loop;     // done flag + sweep index (see loop_graph.h)
+  int sweeps;       // sweeps completed
+  unsigned tick2;   // stage-2 ticket of the grid reduction
 };
 
 struct Scratch {
@@ -120,11 +121,13 @@ struct PullArgs {
   float base_scalar;
   float damping;
   float *score;
-  const float *__restrict__ cin;
-  float *cout;
-  // bins: first block index and first row of each bin
-  int32_t bin_block[kNumBins + 1];
-  int32_t bin_row[kNumBins + 1];
+  // contrib ping-pong: sweep k gathers c[k & 1] and writes c[(k + 1) & 1]
+  float *c0;
+  float *c1;
+  // hub segments (block-cooperative) and warp tasks of bins 1..7
+  int32_t nseg;
+  int32_t task_start[kNumBins + 1];  // first task of bin b; [kNumBins] = total
+  int32_t bin_row[kNumBins + 1];     // first row of bin b; [kNumBins] = n
   const int32_t *__restrict__ seg_row;
   const int32_t *__restrict__ seg_first;
   unsigned *hub_ticket;
@@ -136,7 +139,6 @@ struct PullArgs {
   double *trace;
   SweepCtl *ctl;
   int32_t nblocks;
-  int32_t iter;
   double epsilon;
 };
 
@@ -148,15 +150,19 @@ cudaError_t BuildDeviceGraph(DeviceGraph *g, int64_t n, int64_t m,
                              cudaStream_t s, std::string *err);
 void FreeDeviceGraph(DeviceGraph *g);
 
-int PullBlocks(const DeviceGraph &g, int32_t bin_block[kNumBins + 1]);
+// Warp tasks per bin (fills task_start, returns the total) and the
+// persistent grid size of a sweep kernel (SMs x resident blocks per SM).
+int PullTasks(const DeviceGraph &g, int32_t task_start[kNumBins + 1]);
+int PullGrid(const void *kernel);
 
 cudaError_t LaunchPullInit(const DeviceGraph &g, Scratch &sc, const float *tele_new,
                            float init_scalar, float damping, cudaStream_t s);
-cudaError_t LaunchPullSweep(const PullArgs &a, cudaStream_t s);
+// Kernel to run for one sweep of `a` (a function pointer for LoopGraph).
+const void *PullSweepKernel(const PullArgs &a);
 // Warp-per-row sweep over an arbitrary (unsorted) CSR given in a.rowoff /
 // a.col, a.nblocks blocks, grid-stride; used for adjoint sweeps over the
 // out-rows of directed graphs.
-cudaError_t LaunchPullGeneric(const PullArgs &a, cudaStream_t s);
+const void *PullGenericKernel(const PullArgs &a);
 // Per-edge weight gradient and teleport gradient of the adjoint (pull.cu).
 cudaError_t LaunchAdjointGrads(const DeviceGraph &g, const int32_t *orow, const int32_t *ocol,
                                const float *wout, const float *lam_new, const float *s_new,

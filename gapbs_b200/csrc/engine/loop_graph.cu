@@ -1,0 +1,103 @@
+// loop_graph.cu -- see loop_graph.h.
+#include "loop_graph.h"
+
+#include <cstring>
+
+namespace prgpu {
+
+namespace {
+
+__global__ void loop_decide_kernel(LoopCtl *ctl, int max_iters,
+                                   cudaGraphConditionalHandle cond) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int loops = ctl->loops + 1;
+  ctl->loops = loops;
+  const int go = (ctl->done == 0 && loops < max_iters) ? 1 : 0;
+  cudaGraphSetConditional(cond, static_cast<unsigned>(go));
+}
+
+}  // namespace
+
+void LoopGraph::Reset() {
+  if (exec_) cudaGraphExecDestroy(exec_);
+  exec_ = nullptr;
+  fn_ = nullptr;
+  args_.clear();
+  ctl_ = nullptr;
+  max_iters_ = 0;
+}
+
+cudaError_t LoopGraph::Build(const void *fn, dim3 grid, dim3 block, const void *args,
+                             size_t args_size, LoopCtl *ctl, int max_iters) {
+  Reset();
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e != cudaSuccess) return e;
+  cudaGraphConditionalHandle cond;
+  // The condition starts at 1 on every launch: the body runs at least once.
+  e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNode_t loop_node = nullptr;
+  cudaGraphNodeParams cp = {};
+  if (e == cudaSuccess) {
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&loop_node, g, nullptr, 0, &cp);
+  }
+  if (e == cudaSuccess) {
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    std::vector<unsigned char> arg_copy(static_cast<const unsigned char *>(args),
+                                        static_cast<const unsigned char *>(args) + args_size);
+    void *sweep_params[] = {arg_copy.data()};
+    cudaKernelNodeParams kp = {};
+    kp.func = const_cast<void *>(fn);
+    kp.gridDim = grid;
+    kp.blockDim = block;
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = sweep_params;
+    cudaGraphNode_t sweep_node = nullptr, decide_node = nullptr;
+    e = cudaGraphAddKernelNode(&sweep_node, body, nullptr, 0, &kp);
+    if (e == cudaSuccess) {
+      LoopCtl *c = ctl;
+      int mi = max_iters;
+      cudaGraphConditionalHandle h = cond;
+      void *decide_params[] = {&c, &mi, &h};
+      cudaKernelNodeParams dp = {};
+      dp.func = reinterpret_cast<void *>(loop_decide_kernel);
+      dp.gridDim = dim3(1);
+      dp.blockDim = dim3(32);
+      dp.kernelParams = decide_params;
+      e = cudaGraphAddKernelNode(&decide_node, body, &sweep_node, 1, &dp);
+    }
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec_, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    exec_ = nullptr;
+    return e;
+  }
+  fn_ = fn;
+  grid_ = grid;
+  block_ = block;
+  args_.assign(static_cast<const unsigned char *>(args),
+               static_cast<const unsigned char *>(args) + args_size);
+  ctl_ = ctl;
+  max_iters_ = max_iters;
+  return cudaSuccess;
+}
+
+cudaError_t LoopGraph::Launch(const void *fn, dim3 grid, dim3 block, const void *args,
+                              size_t args_size, LoopCtl *ctl, int max_iters, cudaStream_t s) {
+  if (max_iters < 1) return cudaSuccess;
+  const bool same = exec_ && fn == fn_ && grid.x == grid_.x && block.x == block_.x &&
+                    ctl == ctl_ && max_iters == max_iters_ && args_.size() == args_size &&
+                    std::memcmp(args_.data(), args, args_size) == 0;
+  if (!same) {
+    cudaError_t e = Build(fn, grid, block, args, args_size, ctl, max_iters);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaGraphLaunch(exec_, s);
+}
+
+}  // namespace prgpu

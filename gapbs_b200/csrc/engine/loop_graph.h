@@ -1,0 +1,55 @@
+// loop_graph.h -- a solve's sweep loop as one CUDA graph with a device-side
+// WHILE condition.
+//
+// Body = { sweep kernel, decide kernel }.  The sweep kernel reads the sweep
+// index from LoopCtl::loops and records convergence in LoopCtl::done; the
+// one-thread decide kernel then increments loops and sets the loop condition
+// to (!done && loops < max_iters).  The loop therefore ends after at most
+// max_iters bodies whatever the sweep kernel computes, and no launch is spent
+// after convergence.
+#ifndef GAPBS_B200_ENGINE_LOOP_GRAPH_H_
+#define GAPBS_B200_ENGINE_LOOP_GRAPH_H_
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+namespace prgpu {
+
+// Shared prefix of every solve's device control block.
+struct LoopCtl {
+  int done;   // set by the sweep kernel when the solve converged
+  int loops;  // sweeps issued so far; owned by the decide kernel
+};
+
+class LoopGraph {
+ public:
+  LoopGraph() = default;
+  LoopGraph(const LoopGraph &) = delete;
+  LoopGraph &operator=(const LoopGraph &) = delete;
+  ~LoopGraph() { Reset(); }
+
+  // Launches up to max_iters (>= 1) sweeps of `fn<<<grid, block>>>(args)` on
+  // stream s.  The instantiated graph is cached and reused while the kernel,
+  // launch shape, argument bytes, control block and max_iters are unchanged.
+  cudaError_t Launch(const void *fn, dim3 grid, dim3 block, const void *args,
+                     size_t args_size, LoopCtl *ctl, int max_iters, cudaStream_t s);
+  void Reset();
+
+ private:
+  cudaError_t Build(const void *fn, dim3 grid, dim3 block, const void *args,
+                    size_t args_size, LoopCtl *ctl, int max_iters);
+
+  cudaGraphExec_t exec_ = nullptr;
+  const void *fn_ = nullptr;
+  dim3 grid_, block_;
+  std::vector<unsigned char> args_;
+  LoopCtl *ctl_ = nullptr;
+  int max_iters_ = 0;
+};
+
+}  // namespace prgpu
+
+#endif  // GAPBS_B200_ENGINE_LOOP_GRAPH_H_

@@ -26,6 +26,8 @@ struct pr_gpu {
   bool has_graph = false;
   Scratch sc;
   prgpu::BatchScratch bsc;
+  prgpu::LoopGraph loop_single;   // cached sweep-loop graphs
+  prgpu::LoopGraph loop_adjoint;
   cudaEvent_t ev[4] = {};
   double last_sweep_ms = 0, last_total_ms = 0;
   int64_t last_launches = 0;
@@ -201,8 +203,15 @@ int CheckRunArgs(pr_gpu_t *h, int max_iters, int ncols) {
 int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
                 const float *tele_old, float *out_old, int32_t *sweeps_out, double *err_trace) {
   DeviceGraph &g = h->g;
-  int32_t bin_block[prgpu::kNumBins + 1];
-  const int nblocks = prgpu::PullBlocks(g, bin_block);
+  int32_t task_start[prgpu::kNumBins + 1];
+  prgpu::PullTasks(g, task_start);
+  prgpu::PullArgs probe;
+  std::memset(&probe, 0, sizeof(probe));
+  probe.kind = tele_old ? prgpu::kKindPPR : prgpu::kKindPlain;
+  probe.win = g.weighted ? g.win : nullptr;
+  probe.odeg = (g.directed && !g.weighted) ? g.odeg : nullptr;
+  const void *sweep_fn = prgpu::PullSweepKernel(probe);
+  const int nblocks = prgpu::PullGrid(sweep_fn);
   int rc = EnsureScratch(h, g.n, 1, nblocks, max_iters);
   if (rc) return rc;
   Scratch &sc = h->sc;
@@ -235,9 +244,10 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
   a.damping = damping;
   a.score = sc.score;
   for (int b = 0; b <= prgpu::kNumBins; b++) {
-    a.bin_block[b] = bin_block[b];
+    a.task_start[b] = task_start[b];
     a.bin_row[b] = static_cast<int32_t>(g.bin_row_start[b]);
   }
+  a.nseg = static_cast<int32_t>(g.num_segments);
   a.seg_row = g.seg_row;
   a.seg_first = g.seg_first;
   a.hub_ticket = g.hub_ticket;
@@ -249,14 +259,13 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
   a.ctl = sc.ctl;
   a.nblocks = nblocks;
   a.epsilon = epsilon;
+  a.c0 = sc.contrib[0];
+  a.c1 = sc.contrib[1];
   PR_CHECK(h, cudaEventRecord(h->ev[1], s));
-  for (int it = 0; it < max_iters; it++) {
-    a.iter = it;
-    a.cin = sc.contrib[it & 1];
-    a.cout = sc.contrib[(it + 1) & 1];
-    PR_CHECK(h, prgpu::LaunchPullSweep(a, s));
-    launches += nblocks ? 1 : 0;
-  }
+  if (nblocks > 0)
+    PR_CHECK(h, h->loop_single.Launch(sweep_fn, dim3(nblocks),
+                                      dim3(prgpu::kSweepThreads), &a, sizeof(a), &sc.ctl->loop,
+                                      max_iters, s));
   PR_CHECK(h, cudaEventRecord(h->ev[2], s));
   PR_CHECK(h, prgpu::LaunchGatherOut(g, sc.score, out_old, 1, s));
   launches++;
@@ -273,7 +282,7 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
   cudaEventElapsedTime(&ms_total, h->ev[0], h->ev[3]);
   h->last_sweep_ms = ms_sweep;
   h->last_total_ms = ms_total;
-  h->last_launches = launches;
+  h->last_launches = launches + 2 * static_cast<int64_t>(ctl.loop.loops);  // sweep + decide
   if (sweeps_out) *sweeps_out = max_iters ? ctl.sweeps : 0;
   if (err_trace)
     for (int i = 0; i < max_iters; i++) err_trace[i] = trace[i];
@@ -285,11 +294,15 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
 int SolveAdjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping, const float *w_old,
                  const float *s_old, float *grad_t_old, float *grad_ew) {
   DeviceGraph &g = h->g;
-  int32_t bin_block[prgpu::kNumBins + 1];
+  int32_t task_start[prgpu::kNumBins + 1];
+  prgpu::PullTasks(g, task_start);
   const bool generic = g.directed;
-  int dev_sms = 148;
-  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
-  const int nblocks = generic ? dev_sms * 8 : prgpu::PullBlocks(g, bin_block);
+  prgpu::PullArgs probe;
+  std::memset(&probe, 0, sizeof(probe));
+  probe.kind = prgpu::kKindAdjoint;
+  probe.win = g.weighted ? g.wout : nullptr;
+  const void *adj_fn = generic ? prgpu::PullGenericKernel(probe) : prgpu::PullSweepKernel(probe);
+  const int nblocks = prgpu::PullGrid(adj_fn);
   int rc = EnsureScratch(h, g.n, 1, nblocks, max_iters);
   if (rc) return rc;
   Scratch &sc = h->sc;
@@ -323,9 +336,10 @@ int SolveAdjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping, cons
   a.score = sc.score;
   if (!generic) {
     for (int b = 0; b <= prgpu::kNumBins; b++) {
-      a.bin_block[b] = bin_block[b];
+      a.task_start[b] = task_start[b];
       a.bin_row[b] = static_cast<int32_t>(g.bin_row_start[b]);
     }
+    a.nseg = static_cast<int32_t>(g.num_segments);
     a.seg_row = g.seg_row;
     a.seg_first = g.seg_first;
     a.hub_ticket = g.hub_ticket;
@@ -338,14 +352,12 @@ int SolveAdjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping, cons
   a.ctl = sc.ctl;
   a.nblocks = nblocks;
   a.epsilon = epsilon * wnorm;
+  a.c0 = sc.contrib[0];
+  a.c1 = sc.contrib[1];
   PR_CHECK(h, cudaEventRecord(h->ev[1], s));
-  for (int it = 0; it < max_iters; it++) {
-    a.iter = it;
-    a.cin = sc.contrib[it & 1];
-    a.cout = sc.contrib[(it + 1) & 1];
-    PR_CHECK(h, generic ? prgpu::LaunchPullGeneric(a, s) : prgpu::LaunchPullSweep(a, s));
-    launches++;
-  }
+  if (nblocks > 0)
+    PR_CHECK(h, h->loop_adjoint.Launch(adj_fn, dim3(nblocks), dim3(prgpu::kSweepThreads), &a, sizeof(a),
+                                       &sc.ctl->loop, max_iters, s));
   PR_CHECK(h, cudaEventRecord(h->ev[2], s));
   PR_CHECK(h, prgpu::LaunchAdjointGrads(g, orow, ocol, g.weighted ? g.wout : nullptr, sc.score,
                                         sc.aux[0], damping, grad_ew, grad_t_old, s));
@@ -359,7 +371,7 @@ int SolveAdjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping, cons
   cudaEventElapsedTime(&ms_total, h->ev[0], h->ev[3]);
   h->last_sweep_ms = ms_sweep;
   h->last_total_ms = ms_total;
-  h->last_launches = launches;
+  h->last_launches = launches + 2 * static_cast<int64_t>(ctl.loop.loops);
   h->last_adjoint_sweeps = max_iters ? ctl.sweeps : 0;
   return PR_GPU_OK;
 }
@@ -389,6 +401,8 @@ void pr_gpu_destroy(pr_gpu_t *h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  h->loop_single.Reset();
+  h->loop_adjoint.Reset();
   prgpu::FreeDeviceGraph(&h->g);
   FreeScratch(&h->sc);
   prgpu::FreeBatchScratch(&h->bsc);

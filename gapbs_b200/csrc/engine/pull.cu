@@ -61,32 +61,50 @@ __device__ __forceinline__ float gather_chunk(float acc, const int4 q, const flo
 }
 
 // Sum over entries [s, e) by the calling lane of a G-lane group: the lane
-// takes aligned chunks (s/4 + lane), (s/4 + lane + G), ...; two chunk loads
-// are issued before their gathers.
+// takes aligned 4-entry chunks (s/4 + lane), (s/4 + lane + G), ...; up to four
+// chunk loads are in flight before their gathers are issued.
 template <int G, bool W>
-__device__ __forceinline__ float lane_partial(const PullArgs &a, int s, int e, int lane,
-                                              uint64_t ps, uint64_t pg) {
+__device__ __forceinline__ float lane_partial(const PullArgs &a, const float *cin, int s, int e,
+                                              int lane, uint64_t ps, uint64_t pg) {
   const int4 *col4 = reinterpret_cast<const int4 *>(a.col);
   const float4 *w4 = reinterpret_cast<const float4 *>(a.win);
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int4 zi = make_int4(0, 0, 0, 0);
   float acc = 0.f;
   const int c1 = (e + 3) >> 2;
   int c = (s >> 2) + lane;
-  for (; c + G < c1; c += 2 * G) {
+  for (; c + 3 * G < c1; c += 4 * G) {
     const int4 q0 = ld_stream_v4(col4 + c, ps);
     const int4 q1 = ld_stream_v4(col4 + c + G, ps);
-    float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f), w1 = w0;
+    const int4 q2 = ld_stream_v4(col4 + c + 2 * G, ps);
+    const int4 q3 = ld_stream_v4(col4 + c + 3 * G, ps);
+    float4 w0 = z4, w1 = z4, w2 = z4, w3 = z4;
     if (W) {
       w0 = ld_stream_v4f(w4 + c, ps);
       w1 = ld_stream_v4f(w4 + c + G, ps);
+      w2 = ld_stream_v4f(w4 + c + 2 * G, ps);
+      w3 = ld_stream_v4f(w4 + c + 3 * G, ps);
     }
-    acc = gather_chunk<W>(acc, q0, w0, c << 2, s, e, a.cin, pg);
-    acc = gather_chunk<W>(acc, q1, w1, (c + G) << 2, s, e, a.cin, pg);
+    acc = gather_chunk<W>(acc, q0, w0, c << 2, s, e, cin, pg);
+    acc = gather_chunk<W>(acc, q1, w1, (c + G) << 2, s, e, cin, pg);
+    acc = gather_chunk<W>(acc, q2, w2, (c + 2 * G) << 2, s, e, cin, pg);
+    acc = gather_chunk<W>(acc, q3, w3, (c + 3 * G) << 2, s, e, cin, pg);
   }
   if (c < c1) {
+    // up to three remaining chunks, loads predicated on the row's last chunk
+    const bool h1 = c + G < c1, h2 = c + 2 * G < c1;
     const int4 q0 = ld_stream_v4(col4 + c, ps);
-    float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (W) w0 = ld_stream_v4f(w4 + c, ps);
-    acc = gather_chunk<W>(acc, q0, w0, c << 2, s, e, a.cin, pg);
+    const int4 q1 = h1 ? ld_stream_v4(col4 + c + G, ps) : zi;
+    const int4 q2 = h2 ? ld_stream_v4(col4 + c + 2 * G, ps) : zi;
+    float4 w0 = z4, w1 = z4, w2 = z4;
+    if (W) {
+      w0 = ld_stream_v4f(w4 + c, ps);
+      if (h1) w1 = ld_stream_v4f(w4 + c + G, ps);
+      if (h2) w2 = ld_stream_v4f(w4 + c + 2 * G, ps);
+    }
+    acc = gather_chunk<W>(acc, q0, w0, c << 2, s, e, cin, pg);
+    if (h1) acc = gather_chunk<W>(acc, q1, w1, (c + G) << 2, s, e, cin, pg);
+    if (h2) acc = gather_chunk<W>(acc, q2, w2, (c + 2 * G) << 2, s, e, cin, pg);
   }
   return acc;
 }
@@ -100,27 +118,28 @@ __device__ __forceinline__ float denom_of(const PullArgs &a, int u, int s, int e
 
 // Updates row u from its gathered sum; returns |new - old| (as float).
 template <bool W, bool DIR, int KIND>
-__device__ __forceinline__ float finish_row(const PullArgs &a, int u, int s, int e,
-                                            float sum, uint64_t ps, uint64_t pl) {
-  const float old = ld_score(a.score + u, ps);
+__device__ __forceinline__ float finish_row(const PullArgs &a, float *cout, int u, int s, int e,
+                                            float sum, float old, uint64_t ps, uint64_t pl) {
   const float base = KIND != kKindPlain ? a.base_vec[u] : a.base_scalar;
   if (KIND == kKindAdjoint) {
     // lambda[v] = w[v] + d * (sum_u w(v->u) lambda[u]) / S_v; lambda itself
     // is what the next sweep gathers.
-    const float nw = pr_update(base, a.damping, __fdiv_rn(sum, denom_of<W, DIR>(a, u, s, e)));
+    // A vertex without out-edges has no row in P: (P lambda)[v] = 0.
+    const float den = denom_of<W, DIR>(a, u, s, e);
+    const float nw = pr_update(base, a.damping, den > 0.f ? __fdiv_rn(sum, den) : 0.f);
     st_hint_f32(a.score + u, nw, ps);
-    st_hint_f32(a.cout + u, nw, pl);
+    st_hint_f32(cout + u, nw, pl);
     return fabsf(__fsub_rn(nw, old));
   }
   const float nw = pr_update(base, a.damping, sum);
   st_hint_f32(a.score + u, nw, ps);
-  st_hint_f32(a.cout + u, __fdiv_rn(nw, denom_of<W, DIR>(a, u, s, e)), pl);
+  st_hint_f32(cout + u, __fdiv_rn(nw, denom_of<W, DIR>(a, u, s, e)), pl);
   return fabsf(__fsub_rn(nw, old));
 }
 
 // Deterministic two-stage FP64 grid reduction of the block errors; the last
 // block records the sweep's error and the convergence decision.
-__device__ __forceinline__ void grid_finish(const PullArgs &a, double block_err,
+__device__ __forceinline__ void grid_finish(const PullArgs &a, int it, double block_err,
                                             double *sred) {
   __shared__ int s_last;
   const int b = blockIdx.x;
@@ -154,46 +173,54 @@ __device__ __forceinline__ void grid_finish(const PullArgs &a, double block_err,
   for (int i = threadIdx.x; i < ngroups; i += blockDim.x) v += __ldcg(a.part2 + i);
   tot = block_sum_d<kSweepThreads>(v, sred);
   if (threadIdx.x == 0) {
-    a.trace[a.iter] = tot;
-    a.ctl->sweeps = a.iter + 1;
+    a.trace[it] = tot;
+    a.ctl->sweeps = it + 1;
     a.ctl->tick2 = 0;
-    if (tot < a.epsilon) a.ctl->done = 1;
+    if (tot < a.epsilon) a.ctl->loop.done = 1;
     __threadfence();
   }
 }
 
+// One warp task of a G-lane-group bin: rows bin_row[bin] + task * (32 / G)
+// + lane / G, one row per group.  The group leader's old-score load is issued
+// before the gather so the two latencies overlap.
 template <int G, bool W, bool DIR, int KIND>
-__device__ __forceinline__ float group_rows(const PullArgs &a, int bin, uint64_t ps,
-                                            uint64_t pg, uint64_t pl) {
-  constexpr int kRowsPerBlock = kSweepThreads / G;
-  const int lane = threadIdx.x % G;
-  const int u = a.bin_row[bin] + (blockIdx.x - a.bin_block[bin]) * kRowsPerBlock +
-                static_cast<int>(threadIdx.x) / G;
+__device__ __forceinline__ float warp_task(const PullArgs &a, const float *cin, float *cout,
+                                           int bin, int task, int lane32, uint64_t ps,
+                                           uint64_t pg, uint64_t pl) {
+  constexpr int kRowsPerTask = 32 / G;
+  const int lane = lane32 % G;
+  const int u = a.bin_row[bin] + task * kRowsPerTask + lane32 / G;
   const bool valid = u < a.bin_row[bin + 1];
   int s = 0, e = 0;
+  float old = 0.f;
   if (valid) {
     s = a.rowoff[u];
     e = a.rowoff[u + 1];
+    if (lane == 0) old = ld_score(a.score + u, ps);
   }
-  float acc = lane_partial<G, W>(a, s, e, lane, ps, pg);
+  float acc = lane_partial<G, W>(a, cin, s, e, lane, ps, pg);
   acc = group_sum<G>(acc);
   float err = 0.f;
-  if (valid && lane == 0) err = finish_row<W, DIR, KIND>(a, u, s, e, acc, ps, pl);
+  if (valid && lane == 0) err = finish_row<W, DIR, KIND>(a, cout, u, s, e, acc, old, ps, pl);
   return err;
 }
 
+// One hub segment, processed by the whole block; the block that completes a
+// row's last segment (per-row ticket) sums the row's segment partials in
+// segment order and updates the row.  Called block-uniformly.
 template <bool W, bool DIR, int KIND>
-__device__ __forceinline__ float hub_segment(const PullArgs &a, float *sredf, uint64_t ps,
-                                             uint64_t pg, uint64_t pl) {
+__device__ __forceinline__ float hub_segment(const PullArgs &a, const float *cin, float *cout,
+                                             float *sredf, int seg, uint64_t ps, uint64_t pg,
+                                             uint64_t pl) {
   __shared__ int s_fin;
-  const int seg = blockIdx.x - a.bin_block[kBinHub];
   const int u = a.seg_row[seg];
   const int first = a.seg_first[u];
   const int nseg = a.seg_first[u + 1] - first;
   const int rs = a.rowoff[u], re = a.rowoff[u + 1];
   const int s = rs + (seg - first) * kSegEntries;
   const int e = min(re, s + kSegEntries);
-  float acc = lane_partial<kSweepThreads, W>(a, s, e, threadIdx.x, ps, pg);
+  float acc = lane_partial<kSweepThreads, W>(a, cin, s, e, threadIdx.x, ps, pg);
   const float part = block_sum_f<kSweepThreads>(acc, sredf);
   if (threadIdx.x == 0) {
     a.seg_partial[seg] = part;
@@ -208,61 +235,84 @@ __device__ __forceinline__ float hub_segment(const PullArgs &a, float *sredf, ui
     float sum = 0.f;
     for (int k = 0; k < nseg; k++) sum = __fadd_rn(sum, __ldcg(a.seg_partial + first + k));
     a.hub_ticket[u] = 0;
-    err = finish_row<W, DIR, KIND>(a, u, rs, re, sum, ps, pl);
+    err = finish_row<W, DIR, KIND>(a, cout, u, rs, re, sum, ld_score(a.score + u, ps), ps, pl);
   }
   return err;
 }
 
+// One warp task of the ZERO bin: 32 * kZeroRowsPerThread rows without
+// in-neighbours (new = base).
 template <bool W, bool DIR, int KIND>
-__device__ __forceinline__ float zero_rows(const PullArgs &a, uint64_t ps, uint64_t pl) {
-  constexpr int kRows = kSweepThreads * kZeroRowsPerThread;
-  const int row0 = a.bin_row[kBinZero] + (blockIdx.x - a.bin_block[kBinZero]) * kRows;
+__device__ __forceinline__ float zero_task(const PullArgs &a, float *cout, int task, int lane32,
+                                           uint64_t ps, uint64_t pl) {
+  constexpr int kRows = 32 * kZeroRowsPerThread;
+  const int row0 = a.bin_row[kBinZero] + task * kRows;
   const int end = a.bin_row[kBinZero + 1];
+  float old[kZeroRowsPerThread];
+#pragma unroll
+  for (int i = 0; i < kZeroRowsPerThread; i++) {
+    const int u = row0 + i * 32 + lane32;
+    old[i] = u < end ? ld_score(a.score + u, ps) : 0.f;
+  }
   float err = 0.f;
 #pragma unroll
   for (int i = 0; i < kZeroRowsPerThread; i++) {
-    const int u = row0 + i * kSweepThreads + threadIdx.x;
+    const int u = row0 + i * 32 + lane32;
     if (u < end) {
-      const float old = ld_score(a.score + u, ps);
       const float base = KIND != kKindPlain ? a.base_vec[u] : a.base_scalar;
       const float nw = pr_update(base, a.damping, 0.f);
       st_hint_f32(a.score + u, nw, ps);
       // A row without in-neighbours can still have out-neighbours in a
       // directed graph; its contrib is then read by the next sweep.
-      if (KIND == kKindAdjoint) st_hint_f32(a.cout + u, nw, pl);
-      else if (W || DIR) st_hint_f32(a.cout + u, __fdiv_rn(nw, denom_of<W, DIR>(a, u, 0, 0)), pl);
-      err += fabsf(__fsub_rn(nw, old));
+      if (KIND == kKindAdjoint) st_hint_f32(cout + u, nw, pl);
+      else if (W || DIR) st_hint_f32(cout + u, __fdiv_rn(nw, denom_of<W, DIR>(a, u, 0, 0)), pl);
+      err += fabsf(__fsub_rn(nw, old[i]));
     }
   }
   return err;
 }
 
+// Persistent sweep: every block first takes hub segments (block-cooperative,
+// round-robin), then every warp takes row tasks of bins 1..7 interleaved
+// across all warps of the grid.  Rows are sorted by length, so interleaving
+// hands every warp an even share of each length class.  One block reduction
+// and one grid reduction per sweep.
 template <bool W, bool DIR, int KIND>
 __global__ void __launch_bounds__(kSweepThreads)
 pull_sweep_kernel(const PullArgs a) {
-  if (*reinterpret_cast<volatile const int *>(&a.ctl->done)) return;
+  if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
+  const int it = *reinterpret_cast<volatile const int *>(&a.ctl->loop.loops);
+  const float *cin = (it & 1) ? a.c1 : a.c0;
+  float *cout = (it & 1) ? a.c0 : a.c1;
   __shared__ double sred[kSweepThreads / 32];
   __shared__ float sredf[kSweepThreads / 32];
   const uint64_t ps = policy_evict_first();
   const uint64_t pg = policy_evict_last();
   const uint64_t pl = pg;
-  const int b = blockIdx.x;
-  int bin = 0;
-#pragma unroll
-  for (int i = 1; i < kNumBins; i++) bin += (b >= a.bin_block[i]);
   float err = 0.f;
-  switch (bin) {
-    case 0: err = hub_segment<W, DIR, KIND>(a, sredf, ps, pg, pl); break;
-    case 1: err = group_rows<32, W, DIR, KIND>(a, 1, ps, pg, pl); break;
-    case 2: err = group_rows<16, W, DIR, KIND>(a, 2, ps, pg, pl); break;
-    case 3: err = group_rows<8, W, DIR, KIND>(a, 3, ps, pg, pl); break;
-    case 4: err = group_rows<4, W, DIR, KIND>(a, 4, ps, pg, pl); break;
-    case 5: err = group_rows<2, W, DIR, KIND>(a, 5, ps, pg, pl); break;
-    case 6: err = group_rows<1, W, DIR, KIND>(a, 6, ps, pg, pl); break;
-    default: err = zero_rows<W, DIR, KIND>(a, ps, pl); break;
+  for (int seg = blockIdx.x; seg < a.nseg; seg += gridDim.x)
+    err += hub_segment<W, DIR, KIND>(a, cin, cout, sredf, seg, ps, pg, pl);
+  const int lane32 = threadIdx.x & 31;
+  const int gw = blockIdx.x * (kSweepThreads / 32) + (threadIdx.x >> 5);
+  const int nw = gridDim.x * (kSweepThreads / 32);
+  const int ntasks = a.task_start[kNumBins];
+  for (int t = gw; t < ntasks; t += nw) {
+    int bin = 1;
+#pragma unroll
+    for (int i = 2; i < kNumBins; i++) bin += (t >= a.task_start[i]);
+    const int k = t - a.task_start[bin];
+    switch (bin) {
+      case 1: err += warp_task<32, W, DIR, KIND>(a, cin, cout, 1, k, lane32, ps, pg, pl); break;
+      case 2: err += warp_task<16, W, DIR, KIND>(a, cin, cout, 2, k, lane32, ps, pg, pl); break;
+      case 3: err += warp_task<8, W, DIR, KIND>(a, cin, cout, 3, k, lane32, ps, pg, pl); break;
+      case 4: err += warp_task<4, W, DIR, KIND>(a, cin, cout, 4, k, lane32, ps, pg, pl); break;
+      case 5: err += warp_task<2, W, DIR, KIND>(a, cin, cout, 5, k, lane32, ps, pg, pl); break;
+      case 6: err += warp_task<1, W, DIR, KIND>(a, cin, cout, 6, k, lane32, ps, pg, pl); break;
+      default: err += zero_task<W, DIR, KIND>(a, cout, k, lane32, ps, pl); break;
+    }
   }
   const double block_err = block_sum_d<kSweepThreads>(static_cast<double>(err), sred);
-  grid_finish(a, block_err, sred);
+  grid_finish(a, it, block_err, sred);
 }
 
 // ---- generic warp-per-row sweep (unsorted CSR, grid-stride) ----------------
@@ -270,7 +320,10 @@ pull_sweep_kernel(const PullArgs a) {
 template <bool W, int KIND>
 __global__ void __launch_bounds__(kSweepThreads)
 pull_generic_kernel(const PullArgs a) {
-  if (*reinterpret_cast<volatile const int *>(&a.ctl->done)) return;
+  if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
+  const int it = *reinterpret_cast<volatile const int *>(&a.ctl->loop.loops);
+  const float *cin = (it & 1) ? a.c1 : a.c0;
+  float *cout = (it & 1) ? a.c0 : a.c1;
   __shared__ double sred[kSweepThreads / 32];
   const uint64_t ps = policy_evict_first();
   const uint64_t pg = policy_evict_last();
@@ -279,25 +332,22 @@ pull_generic_kernel(const PullArgs a) {
   float err = 0.f;
   for (int u = blockIdx.x * (kSweepThreads / 32) + (threadIdx.x >> 5); u < a.n; u += warps) {
     const int s = a.rowoff[u], e = a.rowoff[u + 1];
-    float acc = lane_partial<32, W>(a, s, e, lane, ps, pg);
+    float acc = lane_partial<32, W>(a, cin, s, e, lane, ps, pg);
     acc = group_sum<32>(acc);
-    if (lane == 0) err += finish_row<W, false, KIND>(a, u, s, e, acc, ps, pg);
+    if (lane == 0)
+      err += finish_row<W, false, KIND>(a, cout, u, s, e, acc, ld_score(a.score + u, ps), ps, pg);
   }
   const double block_err = block_sum_d<kSweepThreads>(static_cast<double>(err), sred);
-  grid_finish(a, block_err, sred);
+  grid_finish(a, it, block_err, sred);
 }
 
-cudaError_t LaunchPullGeneric(const PullArgs &a, cudaStream_t s) {
-  if (a.nblocks == 0) return cudaSuccess;
+const void *PullGenericKernel(const PullArgs &a) {
   const bool W = a.win != nullptr;
-  if (a.kind == kKindAdjoint) {
-    if (W) pull_generic_kernel<true, kKindAdjoint><<<a.nblocks, kSweepThreads, 0, s>>>(a);
-    else pull_generic_kernel<false, kKindAdjoint><<<a.nblocks, kSweepThreads, 0, s>>>(a);
-  } else {
-    if (W) pull_generic_kernel<true, kKindPPR><<<a.nblocks, kSweepThreads, 0, s>>>(a);
-    else pull_generic_kernel<false, kKindPPR><<<a.nblocks, kSweepThreads, 0, s>>>(a);
-  }
-  return cudaGetLastError();
+  if (a.kind == kKindAdjoint)
+    return W ? reinterpret_cast<const void *>(pull_generic_kernel<true, kKindAdjoint>)
+             : reinterpret_cast<const void *>(pull_generic_kernel<false, kKindAdjoint>);
+  return W ? reinterpret_cast<const void *>(pull_generic_kernel<true, kKindPPR>)
+           : reinterpret_cast<const void *>(pull_generic_kernel<false, kKindPPR>);
 }
 
 // ---- adjoint gradients ---------------------------------------------------------
@@ -412,43 +462,40 @@ __global__ void gather_in_kernel(int32_t n, int ncols, const int32_t *__restrict
 
 // ---- launchers ---------------------------------------------------------------
 
-int PullBlocks(const DeviceGraph &g, int32_t bin_block[kNumBins + 1]) {
-  int64_t blocks = 0;
-  for (int b = 0; b < kNumBins; b++) {
-    bin_block[b] = static_cast<int32_t>(blocks);
+int PullTasks(const DeviceGraph &g, int32_t task_start[kNumBins + 1]) {
+  int64_t tasks = 0;
+  task_start[0] = 0;
+  for (int b = 1; b < kNumBins; b++) {
+    task_start[b] = static_cast<int32_t>(tasks);
     const int64_t rows = g.bin_row_start[b + 1] - g.bin_row_start[b];
-    if (b == kBinHub) {
-      blocks += g.num_segments;
-    } else if (b == kBinZero) {
-      const int64_t per = kSweepThreads * kZeroRowsPerThread;
-      blocks += (rows + per - 1) / per;
-    } else {
-      const int64_t per = kSweepThreads / kBinGroup[b];
-      blocks += (rows + per - 1) / per;
-    }
+    const int64_t per = (b == kBinZero) ? 32 * kZeroRowsPerThread : 32 / kBinGroup[b];
+    tasks += (rows + per - 1) / per;
   }
-  bin_block[kNumBins] = static_cast<int32_t>(blocks);
-  return static_cast<int>(blocks);
+  task_start[kNumBins] = static_cast<int32_t>(tasks);
+  return static_cast<int>(tasks);
 }
 
-cudaError_t LaunchPullSweep(const PullArgs &a, cudaStream_t s) {
-  if (a.nblocks == 0) return cudaSuccess;
-  const bool W = a.win != nullptr, DIR = a.odeg != nullptr;
-  const int kind = a.kind;
-  dim3 grid(a.nblocks), block(kSweepThreads);
-#define PR_LAUNCH(w, d, k) pull_sweep_kernel<w, d, k><<<grid, block, 0, s>>>(a)
-#define PR_KINDS(w, d)                                        \
-  do {                                                        \
-    if (kind == kKindPlain) PR_LAUNCH(w, d, kKindPlain);      \
-    else if (kind == kKindPPR) PR_LAUNCH(w, d, kKindPPR);     \
-    else PR_LAUNCH(w, d, kKindAdjoint);                       \
-  } while (0)
-  if (W) PR_KINDS(true, false);
-  else if (DIR) PR_KINDS(false, true);
-  else PR_KINDS(false, false);
-#undef PR_KINDS
-#undef PR_LAUNCH
-  return cudaGetLastError();
+int PullGrid(const void *kernel) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kSweepThreads, 0) !=
+          cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return sms * per_sm;
+}
+
+template <bool W, bool DIR>
+const void *SweepForKind(int kind) {
+  if (kind == kKindPlain) return reinterpret_cast<const void *>(pull_sweep_kernel<W, DIR, kKindPlain>);
+  if (kind == kKindPPR) return reinterpret_cast<const void *>(pull_sweep_kernel<W, DIR, kKindPPR>);
+  return reinterpret_cast<const void *>(pull_sweep_kernel<W, DIR, kKindAdjoint>);
+}
+
+const void *PullSweepKernel(const PullArgs &a) {
+  if (a.win != nullptr) return SweepForKind<true, false>(a.kind);
+  if (a.odeg != nullptr) return SweepForKind<false, true>(a.kind);
+  return SweepForKind<false, false>(a.kind);
 }
 
 cudaError_t LaunchPullInit(const DeviceGraph &g, Scratch &sc, const float *tele_new,
