@@ -1,11 +1,29 @@
 // loop_graph.cu -- see loop_graph.h.
 #include "loop_graph.h"
 
+#include <cstdlib>
 #include <cstring>
 
 namespace prgpu {
 
 namespace {
+
+// Profilers that replay kernels one by one cannot replay kernel nodes inside
+// a graph with conditional nodes.  GAPBS_PR_PLAIN_LAUNCH=1 makes Launch issue
+// the same kernels as ordinary launches instead: max_iters sweep launches
+// (those after convergence return at once) each followed by a one-thread
+// kernel that advances the sweep index.  Results are identical.
+bool PlainLaunchMode() {
+  static const bool plain = [] {
+    const char *v = std::getenv("GAPBS_PR_PLAIN_LAUNCH");
+    return v && v[0] == '1';
+  }();
+  return plain;
+}
+
+__global__ void loop_advance_kernel(LoopCtl *ctl) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctl->loops = ctl->loops + 1;
+}
 
 __global__ void loop_decide_kernel(LoopCtl *ctl, int max_iters,
                                    cudaGraphConditionalHandle cond) {
@@ -90,6 +108,17 @@ cudaError_t LoopGraph::Build(const void *fn, dim3 grid, dim3 block, const void *
 cudaError_t LoopGraph::Launch(const void *fn, dim3 grid, dim3 block, const void *args,
                               size_t args_size, LoopCtl *ctl, int max_iters, cudaStream_t s) {
   if (max_iters < 1) return cudaSuccess;
+  if (PlainLaunchMode()) {
+    std::vector<unsigned char> blob(static_cast<const unsigned char *>(args),
+                                    static_cast<const unsigned char *>(args) + args_size);
+    void *params[] = {blob.data()};
+    for (int i = 0; i < max_iters; i++) {
+      cudaError_t e = cudaLaunchKernel(fn, grid, block, params, 0, s);
+      if (e != cudaSuccess) return e;
+      loop_advance_kernel<<<1, 32, 0, s>>>(ctl);
+    }
+    return cudaGetLastError();
+  }
   const bool same = exec_ && fn == fn_ && grid.x == grid_.x && block.x == block_.x &&
                     ctl == ctl_ && max_iters == max_iters_ && args_.size() == args_size &&
                     std::memcmp(args_.data(), args, args_size) == 0;
