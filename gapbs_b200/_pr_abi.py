@@ -1,7 +1,7 @@
 """ctypes declarations of include/pr_gpu.h (libgapbs_pr.so)."""
 from __future__ import annotations
 
-from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_void_p
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_void_p
 
 P = c_void_p
 
@@ -17,7 +17,7 @@ PR_GPU_ERANGE = -6
 SYMBOLS = (
     "pr_gpu_create", "pr_gpu_upload", "pr_gpu_run", "pr_gpu_run_device",
     "pr_gpu_adjoint", "pr_gpu_adjoint_device", "pr_gpu_set_stream", "pr_gpu_last_timing",
-    "pr_gpu_graph_info", "pr_gpu_destroy", "pr_gpu_last_error",
+    "pr_gpu_graph_info", "pr_gpu_run_noalloc", "pr_gpu_destroy", "pr_gpu_last_error",
 )
 
 
@@ -41,6 +41,9 @@ def declare(lib):
     lib.pr_gpu_graph_info.argtypes = [P, POINTER(c_int64), POINTER(c_int64), POINTER(c_int64),
                                       POINTER(c_int64), c_int]
     lib.pr_gpu_graph_info.restype = c_int
+    lib.pr_gpu_run_noalloc.argtypes = [c_int, c_int64, c_int64, P, P, P, c_int, c_double, c_float,
+                                       P, P, P, P, c_char_p, c_size_t]
+    lib.pr_gpu_run_noalloc.restype = c_int
     lib.pr_gpu_destroy.argtypes = [P]
     lib.pr_gpu_destroy.restype = None
     lib.pr_gpu_last_error.argtypes = [P]

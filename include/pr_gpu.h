@@ -28,6 +28,7 @@
 #ifndef GAPBS_PR_GPU_H_
 #define GAPBS_PR_GPU_H_
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -128,6 +129,45 @@ int pr_gpu_last_timing(const pr_gpu_t *h, double *sweep_ms, double *total_ms,
  * (nbins entries, bin order as documented in the engine), max in-degree. */
 int pr_gpu_graph_info(const pr_gpu_t *h, int64_t *n, int64_t *m,
                       int64_t *max_degree, int64_t *bin_rows, int nbins);
+
+/* Upper limits of pr_gpu_run_noalloc (sizes of its fixed scratch area). */
+#define PR_GPU_NOALLOC_MAX_VERTICES (1 << 20)
+#define PR_GPU_NOALLOC_MAX_ITERS 1024
+
+/* PageRankPull on a graph that is already in device memory, for callers that
+ * cannot allocate GPU memory: this call makes no cudaMalloc / cudaFree and no
+ * other allocating call.  Typical such callers are applications whose GPU
+ * memory is handed out by their own pool allocator and reserved up front, and
+ * services that must not take the device-wide synchronisation cudaMalloc /
+ * cudaFree can cause while requests are in flight.  It has no counterpart in
+ * the reference (which has no GPU path at all).
+ *
+ * The caller owns every buffer: in_off_dev (n+1) / in_nbr_dev (m) are the
+ * in-CSR (int32, device), out_deg_dev the out-degree per vertex (device;
+ * NULL for an undirected graph, whose in-row length is its out-degree), and
+ * scores_out_dev (n floats, device) receives the scores.  sweeps_out and
+ * err_trace (max_iters doubles) are host pointers and may be NULL.  stream
+ * is a cudaStream_t (NULL = the legacy default stream); the call returns
+ * after the solve.  The result is the reference's PageRankPull (init 1/N,
+ * base (1-d)/N, contrib = score / out-degree, stop when the L1 change of a
+ * sweep < epsilon or after max_iters sweeps) up to FP32 summation order.
+ *
+ * Its working memory is one fixed scratch area compiled into the library
+ * (about 8.4 MB, held on every GPU the library runs on until the process
+ * exits), so n may be at most PR_GPU_NOALLOC_MAX_VERTICES and max_iters at
+ * most PR_GPU_NOALLOC_MAX_ITERS; larger requests return PR_GPU_ERANGE with a
+ * message.  The first call on a device looks up that area's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture
+ * begins.  All calls share the area: calls whose GPU work overlaps in time (several
+ * host threads, or several streams, on one device) race on it and must be
+ * serialised by the caller.  Returns PR_GPU_OK or a PR_GPU_E* code; err_msg
+ * (err_len bytes, nullable) receives a message on failure. */
+int pr_gpu_run_noalloc(int device, int64_t n, int64_t m,
+                       const int32_t *in_off_dev, const int32_t *in_nbr_dev,
+                       const int32_t *out_deg_dev, int max_iters,
+                       double epsilon, float damping, float *scores_out_dev,
+                       int32_t *sweeps_out, double *err_trace, void *stream,
+                       char *err_msg, size_t err_len);
 
 void pr_gpu_destroy(pr_gpu_t *h);
 
