@@ -16,7 +16,8 @@ PR_GPU_ERANGE = -6
 # Every symbol include/pr_gpu.h declares.
 SYMBOLS = (
     "pr_gpu_create", "pr_gpu_upload", "pr_gpu_run", "pr_gpu_run_device",
-    "pr_gpu_adjoint", "pr_gpu_adjoint_device", "pr_gpu_set_stream", "pr_gpu_last_timing",
+    "pr_gpu_adjoint", "pr_gpu_adjoint_device", "pr_gpu_set_stream",
+    "pr_gpu_set_batch_tile", "pr_gpu_get_batch_tile", "pr_gpu_last_timing",
     "pr_gpu_graph_info", "pr_gpu_run_noalloc", "pr_gpu_destroy", "pr_gpu_last_error",
 )
 
@@ -34,6 +35,10 @@ def declare(lib):
     lib.pr_gpu_adjoint.restype = c_int
     lib.pr_gpu_adjoint_device.argtypes = [P, c_int, c_double, c_float, P, P, P, P, P]
     lib.pr_gpu_adjoint_device.restype = c_int
+    lib.pr_gpu_set_batch_tile.argtypes = [P, c_int]
+    lib.pr_gpu_set_batch_tile.restype = c_int
+    lib.pr_gpu_get_batch_tile.argtypes = [P, POINTER(c_int)]
+    lib.pr_gpu_get_batch_tile.restype = c_int
     lib.pr_gpu_set_stream.argtypes = [P, P]
     lib.pr_gpu_set_stream.restype = c_int
     lib.pr_gpu_last_timing.argtypes = [P, POINTER(c_double), POINTER(c_double), POINTER(c_int64)]

@@ -1,17 +1,25 @@
 // batched.cu -- batched personalized PageRank: one launch per sweep updates an
-// N x B block of scores (B <= 64 teleport vectors) as a CSR x dense-block
-// product,
+// N x Bp block of scores (a tile of up to 64 teleport vectors) as a CSR x
+// dense-block product,
 //   S'[u, c] = (1-d) t[u, c] + d * sum_{v in in(u)} S[v, c] / S_v,
 // with a per-column FP64 L1 change and per-column retirement: a column whose
 // change drops below epsilon stops updating (its scores are final) while the
-// others continue.  The block is vertex-major (row u holds its B columns
-// contiguously), so one gathered neighbour row is one or two 128-byte lines
-// and the CSR is streamed once per sweep for all columns.
+// others continue.
 //
-// Work split: hub rows (>= the hub threshold of the plain sweep) are cut into
-// segments, one block per segment, combined by the row's last block in
-// segment order; every other row is handled by one warp whose lanes own
-// columns (lane, lane + 32), round-robin over the degree-sorted rows.
+// Layout: the block is vertex-major (row u holds its Bp columns
+// contiguously, Bp in {8, 16, 32, 64}).  A lane owns four consecutive
+// columns and loads them with one 16-byte load, so L = Bp/4 lanes cover one
+// neighbour row and one warp instruction gathers 32/L neighbour rows, each a
+// whole number of 32-byte sectors.  Four such instructions are in flight per
+// lane before their sums are formed.  The CSR is streamed once per sweep for
+// all Bp columns.  A lane whose four columns have all retired issues no
+// gather, so a sector is skipped once its eight columns have retired.
+//
+// Work split (rows renumbered by descending in-degree, as for the plain
+// sweep): a persistent grid (SMs x resident blocks) first takes the hub-row
+// segments block-cooperatively (the row's last segment block sums the
+// segment partials in segment order), then every warp takes whole rows,
+// interleaved across the grid.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,13 +33,13 @@ namespace prgpu {
 
 namespace {
 
-constexpr int kBT = 256;                 // threads per block
-constexpr int kBW = kBT / 32;            // warps per block
-constexpr int kWarpBlocksPerSM = 8;
+constexpr int kBT = 256;       // threads per block
+constexpr int kBW = kBT / 32;  // warps per block
+constexpr int kUnroll = 4;     // gather instructions in flight per lane
 
 struct BatchArgs {
   int32_t n;
-  int32_t B;
+  int32_t Bp;  // padded tile width
   const int32_t *__restrict__ rowoff;
   const int32_t *__restrict__ col;
   const float *__restrict__ win;
@@ -40,12 +48,11 @@ struct BatchArgs {
   const float *__restrict__ base;
   float damping;
   float *S;
-  float *C0;   // contrib ping-pong: sweep k gathers C[k & 1], writes C[(k + 1) & 1]
+  float *C0;  // contrib ping-pong: sweep k gathers C[k & 1], writes C[(k + 1) & 1]
   float *C1;
   int32_t nseg;
   int32_t hub_rows;
   int32_t zero_start;
-  int32_t warp_blocks;
   const int32_t *__restrict__ seg_row;
   const int32_t *__restrict__ seg_first;
   unsigned *hub_ticket;
@@ -57,7 +64,13 @@ struct BatchArgs {
   double *trace;
   int32_t *sweeps;
   int32_t nblocks;
+  int32_t stop_at;  // stop for a repack once at most this many columns iterate
   double epsilon;
+};
+
+// Tile column c -> caller column (or source column of a repack).
+struct ColMap {
+  int32_t c[kMaxTile];
 };
 
 template <bool W, bool DIR>
@@ -67,106 +80,117 @@ __device__ __forceinline__ float bdenom(const BatchArgs &a, int u) {
   return __int2float_rn(a.rowoff[u + 1] - a.rowoff[u]);
 }
 
-// Warp accumulates sum over entries [s, e) of w_e * Cin[v_e, c] for its two
-// columns; indices are loaded 32 at a time and broadcast by shuffle.
-template <bool W>
-__device__ __forceinline__ void warp_accumulate(const BatchArgs &a, const float *Cin, int s, int e,
-                                                int lane, bool a0, bool a1, float &acc0,
-                                                float &acc1, uint64_t ps, uint64_t pg) {
-  const int B = a.B;
+__device__ __forceinline__ float4 f4add(float4 a, float4 b) {
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+
+// Sum over entries [s, e) of w_e * Cin[v_e, 4*gl .. 4*gl+3], where lane group
+// grp = lane / L takes every (32/L)-th entry; the caller reduces across
+// groups.  Indices (and weights) are loaded 32 at a time and broadcast.
+template <int L, bool W>
+__device__ __forceinline__ float4 row_accumulate(const BatchArgs &a, const float *Cin, int s, int e,
+                                                 int lane, bool gather, uint64_t ps, uint64_t pg,
+                                                 bool have_first = false, int idx_first = 0,
+                                                 float w_first = 0.f) {
+  constexpr int NPW = 32 / L;
+  const int grp = lane / L, gl = lane % L;
+  const int Bp = 4 * L;
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   for (int j0 = s; j0 < e; j0 += 32) {
-    const int j = j0 + lane;
+    const int cnt = min(32, e - j0);
     int idx = 0;
     float w = 0.f;
-    if (j < e) {
-      idx = ld_stream_s32(a.col + j, ps);
-      if (W) w = ld_stream_f32(a.win + j, ps);
+    if (have_first && j0 == s) {
+      idx = idx_first;
+      w = w_first;
+    } else if (lane < cnt) {
+      idx = ld_stream_s32(a.col + j0 + lane, ps);
+      if (W) w = ld_stream_f32(a.win + j0 + lane, ps);
     }
-    const int cnt = min(32, e - j0);
-    int k = 0;
-    for (; k + 4 <= cnt; k += 4) {
-      const int v0 = __shfl_sync(0xffffffffu, idx, k);
-      const int v1 = __shfl_sync(0xffffffffu, idx, k + 1);
-      const int v2 = __shfl_sync(0xffffffffu, idx, k + 2);
-      const int v3 = __shfl_sync(0xffffffffu, idx, k + 3);
-      float w0 = 1.f, w1 = 1.f, w2 = 1.f, w3 = 1.f;
-      if (W) {
-        w0 = __shfl_sync(0xffffffffu, w, k);
-        w1 = __shfl_sync(0xffffffffu, w, k + 1);
-        w2 = __shfl_sync(0xffffffffu, w, k + 2);
-        w3 = __shfl_sync(0xffffffffu, w, k + 3);
+    for (int k = 0; k < cnt; k += NPW * kUnroll) {
+      float4 x[kUnroll];
+      float wk[kUnroll];
+#pragma unroll
+      for (int q = 0; q < kUnroll; q++) {
+        const int kk = k + q * NPW + grp;
+        const int v = __shfl_sync(0xffffffffu, idx, kk & 31);
+        wk[q] = W ? __shfl_sync(0xffffffffu, w, kk & 31) : 1.f;
+        x[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (gather && kk < cnt)
+          x[q] = ld_gather_v4(reinterpret_cast<const float4 *>(Cin + static_cast<int64_t>(v) * Bp) + gl, pg);
       }
-      if (a0) {
-        const float x0 = ld_gather(Cin + static_cast<int64_t>(v0) * B + lane, pg);
-        const float x1 = ld_gather(Cin + static_cast<int64_t>(v1) * B + lane, pg);
-        const float x2 = ld_gather(Cin + static_cast<int64_t>(v2) * B + lane, pg);
-        const float x3 = ld_gather(Cin + static_cast<int64_t>(v3) * B + lane, pg);
+#pragma unroll
+      for (int q = 0; q < kUnroll; q++) {
         if (W) {
-          acc0 = __fmaf_rn(w0, x0, acc0); acc0 = __fmaf_rn(w1, x1, acc0);
-          acc0 = __fmaf_rn(w2, x2, acc0); acc0 = __fmaf_rn(w3, x3, acc0);
+          acc.x = __fmaf_rn(wk[q], x[q].x, acc.x);
+          acc.y = __fmaf_rn(wk[q], x[q].y, acc.y);
+          acc.z = __fmaf_rn(wk[q], x[q].z, acc.z);
+          acc.w = __fmaf_rn(wk[q], x[q].w, acc.w);
         } else {
-          acc0 += x0; acc0 += x1; acc0 += x2; acc0 += x3;
+          acc = f4add(acc, x[q]);
         }
-      }
-      if (a1) {
-        const float x0 = ld_gather(Cin + static_cast<int64_t>(v0) * B + 32 + lane, pg);
-        const float x1 = ld_gather(Cin + static_cast<int64_t>(v1) * B + 32 + lane, pg);
-        const float x2 = ld_gather(Cin + static_cast<int64_t>(v2) * B + 32 + lane, pg);
-        const float x3 = ld_gather(Cin + static_cast<int64_t>(v3) * B + 32 + lane, pg);
-        if (W) {
-          acc1 = __fmaf_rn(w0, x0, acc1); acc1 = __fmaf_rn(w1, x1, acc1);
-          acc1 = __fmaf_rn(w2, x2, acc1); acc1 = __fmaf_rn(w3, x3, acc1);
-        } else {
-          acc1 += x0; acc1 += x1; acc1 += x2; acc1 += x3;
-        }
-      }
-    }
-    for (; k < cnt; k++) {
-      const int v = __shfl_sync(0xffffffffu, idx, k);
-      const float wk = W ? __shfl_sync(0xffffffffu, w, k) : 1.f;
-      if (a0) {
-        const float x = ld_gather(Cin + static_cast<int64_t>(v) * B + lane, pg);
-        acc0 = W ? __fmaf_rn(wk, x, acc0) : acc0 + x;
-      }
-      if (a1) {
-        const float x = ld_gather(Cin + static_cast<int64_t>(v) * B + 32 + lane, pg);
-        acc1 = W ? __fmaf_rn(wk, x, acc1) : acc1 + x;
       }
     }
   }
+  // combine the lane groups (fixed xor order: deterministic)
+#pragma unroll
+  for (int o = L; o < 32; o <<= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+    acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
+    acc.w += __shfl_xor_sync(0xffffffffu, acc.w, o);
+  }
+  return acc;
 }
 
-// Updates column c of row u; returns |new - old|.
-template <bool W, bool DIR>
-__device__ __forceinline__ double bfinish(const BatchArgs &a, float *Cout, int u, int c, float sum,
-                                          float denom, uint64_t ps, uint64_t pl) {
-  const int64_t i = static_cast<int64_t>(u) * a.B + c;
-  const float old = ld_score(a.S + i, ps);
-  const float nw = __fadd_rn(a.base[i], __fmul_rn(a.damping, sum));
-  st_hint_f32(a.S + i, nw, ps);
-  st_hint_f32(Cout + i, __fdiv_rn(nw, denom), pl);
-  return static_cast<double>(fabsf(__fsub_rn(nw, old)));
+__device__ __forceinline__ float comp(const float4 &v, int c) {
+  return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
 }
 
+// Updates the four columns 4*gl.. of row u from their sums (active columns
+// only); adds |new - old| per column to err[].
 template <bool W, bool DIR>
+__device__ __forceinline__ void finish4(const BatchArgs &a, float *Cout, int u, int gl,
+                                        unsigned active4, float4 sum, float4 old, float4 bs,
+                                        float den, double err[4], uint64_t ps, uint64_t pl) {
+  const int64_t i = static_cast<int64_t>(u) * a.Bp + 4 * gl;
+  float nw[4], cv[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const float o = comp(old, c);
+    const bool act = (active4 >> c) & 1u;
+    nw[c] = act ? __fadd_rn(comp(bs, c), __fmul_rn(a.damping, comp(sum, c))) : o;
+    cv[c] = __fdiv_rn(nw[c], den);
+    if (act) err[c] += static_cast<double>(fabsf(__fsub_rn(nw[c], o)));
+  }
+  st_hint_v4(reinterpret_cast<float4 *>(a.S + i), make_float4(nw[0], nw[1], nw[2], nw[3]), ps);
+  st_hint_v4(reinterpret_cast<float4 *>(Cout + i), make_float4(cv[0], cv[1], cv[2], cv[3]), pl);
+}
+
+template <int L, bool W, bool DIR>
 __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
   if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
   const int it = *reinterpret_cast<volatile const int *>(&a.ctl->loop.loops);
   const float *Cin = (it & 1) ? a.C1 : a.C0;
   float *Cout = (it & 1) ? a.C0 : a.C1;
   __shared__ double serr[kBW][kMaxTile];
+  __shared__ double scol[kMaxTile];
   __shared__ float sacc[kBW][kMaxTile];
   __shared__ int s_last;
   const uint64_t ps = policy_evict_first();
   const uint64_t pg = policy_evict_last();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const unsigned long long active = *reinterpret_cast<volatile const unsigned long long *>(&a.ctl->active);
-  const bool a0 = lane < a.B && ((active >> lane) & 1ull);
-  const bool a1 = lane + 32 < a.B && ((active >> (lane + 32)) & 1ull);
-  double e0 = 0, e1 = 0;
-  if (static_cast<int>(blockIdx.x) < a.nseg) {
-    // ---- hub segment: 8 warps split the segment, combine in smem
-    const int seg = blockIdx.x;
+  const int gl = lane % L;
+  const int Bp = a.Bp;
+  const unsigned long long active =
+      *reinterpret_cast<volatile const unsigned long long *>(&a.ctl->active);
+  const unsigned active4 = static_cast<unsigned>((active >> (4 * gl)) & 0xFull);
+  const bool gather = active4 != 0u;
+  double err[4] = {0, 0, 0, 0};
+  if (threadIdx.x < kMaxTile) scol[threadIdx.x] = 0;
+
+  // ---- hub segments, block-cooperative
+  for (int seg = blockIdx.x; seg < a.nseg; seg += gridDim.x) {
     const int u = a.seg_row[seg];
     const int first = a.seg_first[u];
     const int nseg = a.seg_first[u + 1] - first;
@@ -175,15 +199,18 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
     const int e = min(re, s + kSegEntries);
     const int per = (e - s + kBW - 1) / kBW;
     const int ws = min(e, s + wid * per), we = min(e, ws + per);
-    float acc0 = 0.f, acc1 = 0.f;
-    warp_accumulate<W>(a, Cin, ws, we, lane, a0, a1, acc0, acc1, ps, pg);
-    sacc[wid][lane] = acc0;
-    sacc[wid][lane + 32] = acc1;
+    const float4 acc = row_accumulate<L, W>(a, Cin, ws, we, lane, gather, ps, pg);
+    if (lane < L) {
+      sacc[wid][4 * gl + 0] = acc.x;
+      sacc[wid][4 * gl + 1] = acc.y;
+      sacc[wid][4 * gl + 2] = acc.z;
+      sacc[wid][4 * gl + 3] = acc.w;
+    }
     __syncthreads();
-    if (threadIdx.x < a.B) {
+    if (threadIdx.x < Bp) {
       float p = 0.f;
       for (int w = 0; w < kBW; w++) p += sacc[w][threadIdx.x];
-      a.seg_partial[static_cast<int64_t>(seg) * a.B + threadIdx.x] = p;
+      a.seg_partial[static_cast<int64_t>(seg) * Bp + threadIdx.x] = p;
     }
     __threadfence();
     __syncthreads();
@@ -192,46 +219,52 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
       s_last = (t == static_cast<unsigned>(nseg - 1));
     }
     __syncthreads();
-    // The row's last segment block finishes the row: thread c owns column c.
-    double dcol = 0;
     if (s_last) {
+      // the row's last segment block finishes the row: thread c owns column c
       __threadfence();
       const int c = threadIdx.x;
-      if (c < a.B && ((active >> c) & 1ull)) {
+      if (c < Bp && ((active >> c) & 1ull)) {
         float sum = 0.f;
         for (int k = 0; k < nseg; k++)
-          sum = __fadd_rn(sum, __ldcg(a.seg_partial + static_cast<int64_t>(first + k) * a.B + c));
-        dcol = bfinish<W, DIR>(a, Cout, u, c, sum, bdenom<W, DIR>(a, u), ps, pg);
+          sum = __fadd_rn(sum, __ldcg(a.seg_partial + static_cast<int64_t>(first + k) * Bp + c));
+        const int64_t i = static_cast<int64_t>(u) * Bp + c;
+        const float old = ld_score(a.S + i, ps);
+        const float nw = __fadd_rn(a.base[i], __fmul_rn(a.damping, sum));
+        st_hint_f32(a.S + i, nw, ps);
+        st_hint_f32(Cout + i, __fdiv_rn(nw, bdenom<W, DIR>(a, u)), pg);
+        scol[c] += static_cast<double>(fabsf(__fsub_rn(nw, old)));
       }
       if (threadIdx.x == 0) a.hub_ticket[u] = 0;
     }
-    for (int i = threadIdx.x; i < kBW * kMaxTile; i += kBT) (&serr[0][0])[i] = 0;
-    __syncthreads();
-    if (threadIdx.x < kMaxTile) serr[0][threadIdx.x] = dcol;
-    __syncthreads();
-  } else {
-    // ---- warp per row, round-robin over the non-hub rows
-    const int gw = (blockIdx.x - a.nseg) * kBW + wid;
-    const int W_all = a.warp_blocks * kBW;
-    for (int u = a.hub_rows + gw; u < a.n; u += W_all) {
-      float acc0 = 0.f, acc1 = 0.f;
-      if (u < a.zero_start)
-        warp_accumulate<W>(a, Cin, a.rowoff[u], a.rowoff[u + 1], lane, a0, a1, acc0, acc1, ps, pg);
-      const float den = bdenom<W, DIR>(a, u);
-      if (a0) e0 += bfinish<W, DIR>(a, Cout, u, lane, acc0, den, ps, pg);
-      if (a1) e1 += bfinish<W, DIR>(a, Cout, u, lane + 32, acc1, den, ps, pg);
-    }
-    serr[wid][lane] = e0;
-    serr[wid][lane + 32] = e1;
     __syncthreads();
   }
+
+  // ---- every other row: one warp per row, interleaved across the grid
+  const int gw = blockIdx.x * kBW + wid;
+  const int nw = gridDim.x * kBW;
+  for (int u = a.hub_rows + gw; u < a.n; u += nw) {
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (u < a.zero_start)
+      acc = row_accumulate<L, W>(a, Cin, a.rowoff[u], a.rowoff[u + 1], lane, gather, ps, pg);
+    if (lane < L && gather) {
+      const int64_t i = static_cast<int64_t>(u) * Bp + 4 * gl;
+      const float4 old = ld_score_v4(reinterpret_cast<const float4 *>(a.S + i), ps);
+      const float4 bs = *reinterpret_cast<const float4 *>(a.base + i);
+      finish4<W, DIR>(a, Cout, u, gl, active4, acc, old, bs, bdenom<W, DIR>(a, u), err, ps, pg);
+    }
+  }
+
   // ---- per-column block partial, then two-stage grid reduction per column
-  const int B = a.B;
+  if (lane < L) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) serr[wid][4 * gl + c] = err[c];
+  }
+  __syncthreads();
   const int b = blockIdx.x;
-  if (threadIdx.x < B) {
-    double p = 0;
+  if (threadIdx.x < Bp) {
+    double p = scol[threadIdx.x];
     for (int w = 0; w < kBW; w++) p += serr[w][threadIdx.x];
-    a.part1[static_cast<int64_t>(b) * B + threadIdx.x] = p;
+    a.part1[static_cast<int64_t>(b) * Bp + threadIdx.x] = p;
   }
   __threadfence();
   __syncthreads();
@@ -245,11 +278,11 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  if (threadIdx.x < B) {
+  if (threadIdx.x < Bp) {
     double p = 0;
     for (int i = 0; i < gsize; i++)
-      p += __ldcg(a.part1 + static_cast<int64_t>(g * kReduceGroup + i) * B + threadIdx.x);
-    a.part2[static_cast<int64_t>(g) * B + threadIdx.x] = p;
+      p += __ldcg(a.part1 + static_cast<int64_t>(g * kReduceGroup + i) * Bp + threadIdx.x);
+    a.part2[static_cast<int64_t>(g) * Bp + threadIdx.x] = p;
   }
   __threadfence();
   __syncthreads();
@@ -264,10 +297,11 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
   __shared__ unsigned long long s_retire;
   if (threadIdx.x == 0) s_retire = 0ull;
   __syncthreads();
-  if (threadIdx.x < B && ((active >> threadIdx.x) & 1ull)) {
+  if (threadIdx.x < Bp && ((active >> threadIdx.x) & 1ull)) {
     double tot = 0;
-    for (int i = 0; i < ngroups; i++) tot += __ldcg(a.part2 + static_cast<int64_t>(i) * B + threadIdx.x);
-    a.trace[static_cast<int64_t>(it) * B + threadIdx.x] = tot;
+    for (int i = 0; i < ngroups; i++)
+      tot += __ldcg(a.part2 + static_cast<int64_t>(i) * Bp + threadIdx.x);
+    a.trace[static_cast<int64_t>(it) * Bp + threadIdx.x] = tot;
     a.sweeps[threadIdx.x] = it + 1;
     if (tot < a.epsilon) atomicOr(&s_retire, 1ull << threadIdx.x);
   }
@@ -276,20 +310,56 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
     const unsigned long long next = active & ~s_retire;
     a.ctl->active = next;
     a.ctl->tick2 = 0;
-    if (next == 0ull) a.ctl->loop.done = 1;
+    if (next == 0ull) {
+      a.ctl->loop.done = 1;
+    } else if (__popcll(next) <= a.stop_at) {
+      // few enough survivors to repack them into a narrower tile
+      a.ctl->compact = 1;
+      a.ctl->loop.done = 1;
+    }
     __threadfence();
   }
 }
 
+// Copies the surviving columns map.c[j] (j < nact) of a width-Bo tile into
+// columns j of a width-Bn tile (padding columns zero).
+__global__ void batch_repack_kernel(int32_t n, int Bo, int Bn, int nact, ColMap map,
+                                    const float *__restrict__ So, const float *__restrict__ bo,
+                                    const float *__restrict__ Co, float *Sn, float *bn, float *Cn) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<int64_t>(n) * Bn) return;
+  const int64_t u = i / Bn;
+  const int j = static_cast<int>(i - u * Bn);
+  if (j >= nact) {
+    Sn[i] = 0.f;
+    bn[i] = 0.f;
+    Cn[i] = 0.f;
+    return;
+  }
+  const int64_t src = u * Bo + map.c[j];
+  Sn[i] = So[src];
+  bn[i] = bo[src];
+  Cn[i] = Co[src];
+}
+
+// Tile init: S = t, base = (1-d) t, C = t / S_v for the tile's real columns;
+// padding columns are zero.
 template <bool W, bool DIR>
-__global__ void batch_init_kernel(int32_t n, int B, int K, int c0, const int32_t *__restrict__ perm,
+__global__ void batch_init_kernel(int32_t n, int B, int Bp, int K, int c0,
+                                  const int32_t *__restrict__ perm,
                                   const int32_t *__restrict__ rowoff, const int32_t *__restrict__ odeg,
                                   const float *__restrict__ rsum, const float *__restrict__ tele_old,
                                   float uniform, float one_minus_d, float *S, float *C, float *base) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= static_cast<int64_t>(n) * B) return;
-  const int64_t u = i / B;
-  const int c = static_cast<int>(i - u * B);
+  if (i >= static_cast<int64_t>(n) * Bp) return;
+  const int64_t u = i / Bp;
+  const int c = static_cast<int>(i - u * Bp);
+  if (c >= B) {
+    S[i] = 0.f;
+    base[i] = 0.f;
+    C[i] = 0.f;
+    return;
+  }
   const float t = tele_old ? tele_old[static_cast<int64_t>(perm[u]) * K + c0 + c] : uniform;
   float denom;
   if (W) denom = rsum[u];
@@ -300,13 +370,15 @@ __global__ void batch_init_kernel(int32_t n, int B, int K, int c0, const int32_t
   C[i] = __fdiv_rn(t, denom);
 }
 
-__global__ void batch_out_kernel(int32_t n, int B, int K, int c0, const int32_t *__restrict__ inv,
-                                 const float *__restrict__ S, float *out_old) {
+// Writes tile columns j < B (caller column map.c[j]) back in original ids.
+__global__ void batch_out_kernel(int32_t n, int B, int Bp, int K, ColMap map,
+                                 const int32_t *__restrict__ inv, const float *__restrict__ S,
+                                 float *out_old) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= static_cast<int64_t>(n) * B) return;
   const int64_t v = i / B;
-  const int c = static_cast<int>(i - v * B);
-  out_old[v * K + c0 + c] = S[static_cast<int64_t>(inv[v]) * B + c];
+  const int j = static_cast<int>(i - v * B);
+  out_old[v * K + map.c[j]] = S[static_cast<int64_t>(inv[v]) * Bp + j];
 }
 
 template <typename T>
@@ -320,11 +392,279 @@ cudaError_t GrowB(T **p, int64_t *cap, int64_t need) {
   return e;
 }
 
+int PadWidth(int b) {
+  for (int w : kTileWidths)
+    if (b <= w) return w;
+  return kMaxTile;
+}
+
+template <int L>
+const void *SweepFor(const DeviceGraph &g) {
+  if (g.weighted) return reinterpret_cast<const void *>(batch_sweep_kernel<L, true, false>);
+  if (g.directed) return reinterpret_cast<const void *>(batch_sweep_kernel<L, false, true>);
+  return reinterpret_cast<const void *>(batch_sweep_kernel<L, false, false>);
+}
+
+const void *BatchSweepKernel(const DeviceGraph &g, int Bp) {
+  switch (Bp) {
+    case 8: return SweepFor<2>(g);
+    case 16: return SweepFor<4>(g);
+    case 32: return SweepFor<8>(g);
+    default: return SweepFor<16>(g);
+  }
+}
+
+int GridFor(const void *fn) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBT, 0) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  return sms * per_sm;
+}
+
+#define PB_TRY(expr)                                                   \
+  do {                                                                 \
+    cudaError_t e_ = (expr);                                           \
+    if (e_ != cudaSuccess) {                                           \
+      *err = std::string(#expr) + ": " + cudaGetErrorString(e_);       \
+      return e_;                                                       \
+    }                                                                  \
+  } while (0)
+
+// Buffers for tiles up to kMaxTile columns and a grid of up to nblocks.
+cudaError_t EnsureBatchBuffers(const DeviceGraph &g, BatchScratch &bs, int nblocks, int iters,
+                               std::string *err) {
+  const int64_t n = g.n;
+  const int64_t cells = n * kMaxTile;
+  if (!bs.S || bs.cap_cells < cells) {
+    int64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+    for (float **p : {&bs.S, &bs.C[0], &bs.C[1], &bs.base}) {
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+    }
+    bs.cap_cells = 0;
+    PB_TRY(GrowB(&bs.S, &c0, cells));
+    PB_TRY(GrowB(&bs.C[0], &c1, cells));
+    PB_TRY(GrowB(&bs.C[1], &c2, cells));
+    PB_TRY(GrowB(&bs.base, &c3, cells));
+    bs.cap_cells = cells;
+  }
+  const int ngroups = (nblocks + kReduceGroup - 1) / kReduceGroup;
+  PB_TRY(GrowB(&bs.part1, &bs.cap_part, static_cast<int64_t>(nblocks) * kMaxTile));
+  if (!bs.part2 || bs.cap_groups < ngroups + 1) {
+    int64_t c = 0;
+    if (bs.part2) cudaFree(bs.part2), bs.part2 = nullptr;
+    if (bs.tick1) cudaFree(bs.tick1), bs.tick1 = nullptr;
+    PB_TRY(GrowB(&bs.part2, &c, static_cast<int64_t>(ngroups + 1) * kMaxTile));
+    c = 0;
+    PB_TRY(GrowB(&bs.tick1, &c, ngroups + 1));
+    bs.cap_groups = ngroups + 1;
+  }
+  PB_TRY(GrowB(&bs.trace, &bs.cap_trace, static_cast<int64_t>(std::max(iters, 1)) * kMaxTile));
+  if (!bs.sweeps) PB_TRY(cudaMalloc(&bs.sweeps, sizeof(int32_t) * kMaxTile));
+  PB_TRY(GrowB(&bs.seg_partial, &bs.cap_seg, std::max<int64_t>(g.num_segments, 1) * kMaxTile));
+  if (!bs.ctl) PB_TRY(cudaMalloc(&bs.ctl, sizeof(BatchCtl)));
+  return cudaSuccess;
+}
+
+int WidthIndex(int Bp) { return Bp == 8 ? 0 : Bp == 16 ? 1 : Bp == 32 ? 2 : 3; }
+
+// One tile: columns [c0, c0 + B) of the caller's N x K teleport block.
+// The tile iterates in phases: whenever the columns still iterating fit in
+// half the tile width, the loop stops, the survivors are repacked into the
+// narrowest tile that holds them, and sweeping resumes there (retired
+// columns' scores are written out at the end of the phase they retired in).
+cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, int max_iters,
+                      double epsilon, float damping, int K, int c0, int B, int Bp,
+                      const float *tele_old, float *out_old, int32_t *sweeps_tile,
+                      double *trace_tile, float *sweep_ms, int64_t *launches, std::string *err) {
+  const int64_t n = g.n;
+  const int T = 256;
+  const void *fn0 = BatchSweepKernel(g, Bp);
+  const int nblocks0 = GridFor(fn0);
+  PB_TRY(EnsureBatchBuffers(g, bs, nblocks0, max_iters, err));
+  const unsigned ib = static_cast<unsigned>((n * Bp + T - 1) / T);
+  const float uniform = 1.0f / static_cast<float>(n);
+  const float omd = 1.0f - damping;
+  if (g.weighted)
+    batch_init_kernel<true, false><<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, Bp, K, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base);
+  else if (g.directed)
+    batch_init_kernel<false, true><<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, Bp, K, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base);
+  else
+    batch_init_kernel<false, false><<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, Bp, K, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base);
+  PB_TRY(cudaGetLastError());
+  *launches += 1;
+
+  // tile column -> caller column
+  ColMap map;
+  for (int j = 0; j < kMaxTile; j++) map.c[j] = j < B ? c0 + j : 0;
+  int nact = B;                 // columns of the current tile (all iterate at phase start)
+  float *S = bs.S, *base = bs.base;
+  float *Cpair[2] = {bs.C[0], bs.C[1]};  // Cpair[k & 1] is gathered by sweep k
+  int loops = 0;
+  for (int j = 0; j < B; j++) sweeps_tile[j] = 0;
+  std::vector<int32_t> sw(kMaxTile);
+  std::vector<double> tr(static_cast<size_t>(std::max(max_iters, 1)) * kMaxTile);
+  *sweep_ms = 0;
+  cudaEvent_t e0, e1;
+  PB_TRY(cudaEventCreate(&e0));
+  PB_TRY(cudaEventCreate(&e1));
+  int tile_bp = Bp;
+  while (true) {
+    const void *fn = BatchSweepKernel(g, tile_bp);
+    const int nblocks = GridFor(fn);
+    PB_TRY(EnsureBatchBuffers(g, bs, nblocks, max_iters, err));
+    const int ngroups = (nblocks + kReduceGroup - 1) / kReduceGroup;
+    BatchCtl ctl0;
+    std::memset(&ctl0, 0, sizeof(ctl0));
+    ctl0.active = (nact == 64) ? ~0ull : ((1ull << nact) - 1ull);
+    ctl0.loop.done = (loops >= max_iters) ? 1 : 0;
+    ctl0.loop.loops = loops;
+    PB_TRY(cudaMemcpyAsync(bs.ctl, &ctl0, sizeof(ctl0), cudaMemcpyHostToDevice, s));
+    PB_TRY(cudaMemsetAsync(bs.tick1, 0, sizeof(unsigned) * (ngroups + 1), s));
+    PB_TRY(cudaMemsetAsync(bs.sweeps, 0, sizeof(int32_t) * kMaxTile, s));
+    if (max_iters)
+      PB_TRY(cudaMemsetAsync(bs.trace, 0, sizeof(double) * static_cast<int64_t>(max_iters) * kMaxTile, s));
+    BatchArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.n = static_cast<int32_t>(n);
+    a.Bp = tile_bp;
+    a.rowoff = g.rowoff;
+    a.col = g.col;
+    a.win = g.weighted ? g.win : nullptr;
+    a.odeg = g.odeg;
+    a.rsum = g.rsum;
+    a.base = base;
+    a.damping = damping;
+    a.S = S;
+    a.C0 = Cpair[0];
+    a.C1 = Cpair[1];
+    a.nseg = static_cast<int32_t>(g.num_segments);
+    a.hub_rows = static_cast<int32_t>(g.num_hub_rows);
+    a.zero_start = static_cast<int32_t>(g.bin_row_start[kBinZero]);
+    a.seg_row = g.seg_row;
+    a.seg_first = g.seg_first;
+    a.hub_ticket = g.hub_ticket;
+    a.seg_partial = bs.seg_partial;
+    a.part1 = bs.part1;
+    a.part2 = bs.part2;
+    a.tick1 = bs.tick1;
+    a.ctl = bs.ctl;
+    a.trace = bs.trace;
+    a.sweeps = bs.sweeps;
+    a.nblocks = nblocks;
+    a.stop_at = tile_bp > 8 ? tile_bp / 2 : 0;
+    a.epsilon = epsilon;
+    PB_TRY(cudaEventRecord(e0, s));
+    PB_TRY(bs.loop[WidthIndex(tile_bp)].Launch(fn, dim3(nblocks), dim3(kBT), &a, sizeof(a),
+                                               &bs.ctl->loop, max_iters, s));
+    PB_TRY(cudaEventRecord(e1, s));
+    BatchCtl ctl;
+    PB_TRY(cudaMemcpyAsync(&ctl, bs.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+    PB_TRY(cudaMemcpyAsync(sw.data(), bs.sweeps, sizeof(int32_t) * nact, cudaMemcpyDeviceToHost, s));
+    if (max_iters && trace_tile)
+      PB_TRY(cudaMemcpyAsync(tr.data(), bs.trace,
+                             sizeof(double) * static_cast<int64_t>(max_iters) * tile_bp,
+                             cudaMemcpyDeviceToHost, s));
+    // every column of this phase leaves its scores in the caller's block; a
+    // column still iterating is overwritten by a later phase
+    if (out_old) {
+      batch_out_kernel<<<static_cast<unsigned>((n * nact + T - 1) / T), T, 0, s>>>(
+          static_cast<int32_t>(n), nact, tile_bp, K, map, g.inv, S, out_old);
+      PB_TRY(cudaGetLastError());
+      *launches += 1;
+    }
+    PB_TRY(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    *sweep_ms += ms;
+    const int phase_loops = ctl.loop.loops;  // sweeps issued so far (all phases)
+    *launches += 2 * static_cast<int64_t>(phase_loops - loops);
+    for (int j = 0; j < nact; j++) {
+      const int lc = map.c[j] - c0;       // column within the tile
+      if (sw[j] > 0) sweeps_tile[lc] = sw[j];
+      if (trace_tile)
+        for (int it = loops; it < std::min(phase_loops, max_iters); it++)
+          trace_tile[static_cast<int64_t>(it) * kMaxTile + lc] = tr[static_cast<int64_t>(it) * tile_bp + j];
+    }
+    loops = phase_loops;
+    if (!ctl.compact || loops >= max_iters) break;
+    // repack the survivors into the narrowest tile that holds them
+    ColMap src, next_map;
+    int m2 = 0;
+    for (int j = 0; j < nact; j++)
+      if ((ctl.active >> j) & 1ull) {
+        src.c[m2] = j;
+        next_map.c[m2] = map.c[j];
+        m2++;
+      }
+    for (int j = m2; j < kMaxTile; j++) src.c[j] = next_map.c[j] = 0;
+    const int bn = PadWidth(m2);
+    if (!bs.S2) {
+      int64_t c2a = 0, c2b = 0;
+      PB_TRY(GrowB(&bs.S2, &c2a, n * kMaxTile));
+      PB_TRY(GrowB(&bs.base2, &c2b, n * kMaxTile));
+      bs.cap_cells2 = n * kMaxTile;
+    }
+    float *S_new = (S == bs.S) ? bs.S2 : bs.S;
+    float *b_new = (base == bs.base) ? bs.base2 : bs.base;
+    float *C_cur = Cpair[loops & 1];
+    float *C_new = Cpair[(loops + 1) & 1];  // free: holds contribs two sweeps old
+    batch_repack_kernel<<<static_cast<unsigned>((n * bn + T - 1) / T), T, 0, s>>>(
+        static_cast<int32_t>(n), tile_bp, bn, m2, src, S, base, C_cur, S_new, b_new, C_new);
+    PB_TRY(cudaGetLastError());
+    *launches += 1;
+    S = S_new;
+    base = b_new;
+    Cpair[loops & 1] = C_new;
+    Cpair[(loops + 1) & 1] = C_cur;
+    map = next_map;
+    nact = m2;
+    tile_bp = bn;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return cudaSuccess;
+}
+
+// Autotuner: runs two sweeps of the first tile at each supported width and
+// keeps the width with the lowest time per column-sweep.
+cudaError_t TuneTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, float damping,
+                     int ncols, const float *tele_old, std::string *err) {
+  double best = 1e300;
+  int best_w = kMaxTile;
+  std::vector<int32_t> sw(kMaxTile);
+  for (int w : kTileWidths) {
+    const int B = std::min(w, ncols);
+    if (PadWidth(B) != w) continue;  // would waste a wider tile
+    float ms = 0;
+    int64_t nl = 0;
+    // one warm sweep (graph build), then a timed two-sweep solve
+    cudaError_t e = SolveTile(g, bs, s, 1, 0.0, damping, ncols, 0, B, w, tele_old, nullptr,
+                              sw.data(), nullptr, &ms, &nl, err);
+    if (e != cudaSuccess) return e;
+    e = SolveTile(g, bs, s, 2, 0.0, damping, ncols, 0, B, w, tele_old, nullptr, sw.data(),
+                  nullptr, &ms, &nl, err);
+    if (e != cudaSuccess) return e;
+    const double per_col_sweep = ms / (2.0 * B);
+    if (per_col_sweep < best) {
+      best = per_col_sweep;
+      best_w = w;
+    }
+  }
+  bs.tuned_tile = best_w;
+  bs.tuned_ncols = ncols;
+  bs.tuned_graph = g.rowoff;
+  return cudaSuccess;
+}
+
 }  // namespace
 
 void FreeBatchScratch(BatchScratch *b) {
-  b->loop.Reset();
-  float **fp[] = {&b->S, &b->C[0], &b->C[1], &b->base, &b->seg_partial};
+  for (auto &l : b->loop) l.Reset();
+  float **fp[] = {&b->S, &b->C[0], &b->C[1], &b->base, &b->S2, &b->base2, &b->seg_partial};
   for (float **p : fp) {
     if (*p) cudaFree(*p);
     *p = nullptr;
@@ -340,153 +680,56 @@ void FreeBatchScratch(BatchScratch *b) {
   b->tick1 = nullptr;
   b->sweeps = nullptr;
   b->ctl = nullptr;
-  b->cap_cells = b->cap_part = b->cap_trace = b->cap_seg = 0;
+  b->cap_cells = b->cap_cells2 = b->cap_part = b->cap_groups = b->cap_trace = b->cap_seg = 0;
+  b->tuned_tile = b->tuned_ncols = 0;
+  b->tuned_graph = nullptr;
 }
-
-#define PB_TRY(expr)                                                   \
-  do {                                                                 \
-    cudaError_t e_ = (expr);                                           \
-    if (e_ != cudaSuccess) {                                           \
-      *err = std::string(#expr) + ": " + cudaGetErrorString(e_);       \
-      return e_;                                                       \
-    }                                                                  \
-  } while (0)
 
 cudaError_t SolveBatched(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s,
                          int max_iters, double epsilon, float damping, int ncols,
                          const float *tele_old, float *out_old, int32_t *sweeps_out,
                          double *err_trace, double *ms_sweep, double *ms_total,
                          int64_t *launches, std::string *err) {
-  const int tile = bs.tile > 0 ? std::min(bs.tile, kMaxTile) : kMaxTile;
-  const int64_t n = g.n;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int nseg = static_cast<int>(g.num_segments);
-  const int warp_blocks = sms * kWarpBlocksPerSM;
-  const int nblocks = nseg + warp_blocks;
-  const int ngroups = (nblocks + kReduceGroup - 1) / kReduceGroup;
-  const int Bmax = std::min(tile, ncols);
-  PB_TRY(GrowB(&bs.S, &bs.cap_cells, n * Bmax));
-  {
-    int64_t c1 = 0, c2 = 0, c3 = 0;
-    if (bs.C[0]) cudaFree(bs.C[0]), bs.C[0] = nullptr;
-    if (bs.C[1]) cudaFree(bs.C[1]), bs.C[1] = nullptr;
-    if (bs.base) cudaFree(bs.base), bs.base = nullptr;
-    PB_TRY(GrowB(&bs.C[0], &c1, n * Bmax));
-    PB_TRY(GrowB(&bs.C[1], &c2, n * Bmax));
-    PB_TRY(GrowB(&bs.base, &c3, n * Bmax));
+  int tile = bs.tile;
+  if (tile == 0) {
+    if (bs.tuned_graph != g.rowoff || bs.tuned_ncols != ncols || bs.tuned_tile == 0) {
+      cudaError_t e = TuneTile(g, bs, s, damping, ncols, tele_old, err);
+      if (e != cudaSuccess) return e;
+    }
+    tile = bs.tuned_tile;
   }
-  {
-    int64_t c1 = 0, c2 = 0, c3 = 0;
-    if (bs.part1) cudaFree(bs.part1), bs.part1 = nullptr;
-    if (bs.part2) cudaFree(bs.part2), bs.part2 = nullptr;
-    if (bs.tick1) cudaFree(bs.tick1), bs.tick1 = nullptr;
-    PB_TRY(GrowB(&bs.part1, &c1, static_cast<int64_t>(nblocks) * Bmax));
-    PB_TRY(GrowB(&bs.part2, &c2, static_cast<int64_t>(ngroups) * Bmax));
-    PB_TRY(GrowB(&bs.tick1, &c3, ngroups + 1));
-    bs.cap_part = nblocks;
-  }
-  PB_TRY(GrowB(&bs.trace, &bs.cap_trace, static_cast<int64_t>(std::max(max_iters, 1)) * Bmax));
-  {
-    int64_t c = 0;
-    if (bs.sweeps) cudaFree(bs.sweeps), bs.sweeps = nullptr;
-    PB_TRY(GrowB(&bs.sweeps, &c, kMaxTile));
-  }
-  PB_TRY(GrowB(&bs.seg_partial, &bs.cap_seg, std::max<int64_t>(nseg, 1) * Bmax));
-  if (!bs.ctl) PB_TRY(cudaMalloc(&bs.ctl, sizeof(BatchCtl)));
-
-  cudaEvent_t ev[4];
-  for (auto &e : ev) PB_TRY(cudaEventCreate(&e));
-  float sweep_total = 0;
-  int64_t nl = 0;
-  PB_TRY(cudaEventRecord(ev[0], s));
-  const float uniform = 1.0f / static_cast<float>(n);
-  const float omd = 1.0f - damping;
-  std::vector<double> trace_tile(static_cast<size_t>(std::max(max_iters, 1)) * Bmax);
+  tile = PadWidth(std::max(1, std::min(tile, kMaxTile)));
+  cudaEvent_t t0, t1;
+  PB_TRY(cudaEventCreate(&t0));
+  PB_TRY(cudaEventCreate(&t1));
+  PB_TRY(cudaEventRecord(t0, s));
+  std::vector<double> trace_tile(static_cast<size_t>(std::max(max_iters, 1)) * kMaxTile);
   std::vector<int32_t> sweeps_tile(kMaxTile);
+  double sweep_total = 0;
+  int64_t nl = 0;
   for (int c0 = 0; c0 < ncols; c0 += tile) {
     const int B = std::min(tile, ncols - c0);
-    const int T = 256;
-    const unsigned ib = static_cast<unsigned>((n * B + T - 1) / T);
-    if (g.weighted)
-      batch_init_kernel<true, false><<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, ncols, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base);
-    else if (g.directed)
-      batch_init_kernel<false, true><<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, ncols, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base);
-    else
-      batch_init_kernel<false, false><<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, ncols, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base);
-    nl++;
-    BatchCtl ctl0;
-    std::memset(&ctl0, 0, sizeof(ctl0));
-    ctl0.active = (B == 64) ? ~0ull : ((1ull << B) - 1ull);
-    ctl0.loop.done = max_iters == 0 ? 1 : 0;
-    PB_TRY(cudaMemcpyAsync(bs.ctl, &ctl0, sizeof(ctl0), cudaMemcpyHostToDevice, s));
-    PB_TRY(cudaMemsetAsync(bs.tick1, 0, sizeof(unsigned) * (ngroups + 1), s));
-    PB_TRY(cudaMemsetAsync(bs.sweeps, 0, sizeof(int32_t) * kMaxTile, s));
-    if (max_iters)
-      PB_TRY(cudaMemsetAsync(bs.trace, 0, sizeof(double) * static_cast<int64_t>(max_iters) * B, s));
-    BatchArgs a;
-    std::memset(&a, 0, sizeof(a));
-    a.n = static_cast<int32_t>(n);
-    a.B = B;
-    a.rowoff = g.rowoff;
-    a.col = g.col;
-    a.win = g.weighted ? g.win : nullptr;
-    a.odeg = g.odeg;
-    a.rsum = g.rsum;
-    a.base = bs.base;
-    a.damping = damping;
-    a.S = bs.S;
-    a.nseg = nseg;
-    a.hub_rows = static_cast<int32_t>(g.num_hub_rows);
-    a.zero_start = static_cast<int32_t>(g.bin_row_start[kBinZero]);
-    a.warp_blocks = warp_blocks;
-    a.seg_row = g.seg_row;
-    a.seg_first = g.seg_first;
-    a.hub_ticket = g.hub_ticket;
-    a.seg_partial = bs.seg_partial;
-    a.part1 = bs.part1;
-    a.part2 = bs.part2;
-    a.tick1 = bs.tick1;
-    a.ctl = bs.ctl;
-    a.trace = bs.trace;
-    a.sweeps = bs.sweeps;
-    a.nblocks = nblocks;
-    a.epsilon = epsilon;
-    a.C0 = bs.C[0];
-    a.C1 = bs.C[1];
-    const void *fn = g.weighted ? reinterpret_cast<const void *>(batch_sweep_kernel<true, false>)
-                   : g.directed ? reinterpret_cast<const void *>(batch_sweep_kernel<false, true>)
-                                : reinterpret_cast<const void *>(batch_sweep_kernel<false, false>);
-    PB_TRY(cudaEventRecord(ev[1], s));
-    PB_TRY(bs.loop.Launch(fn, dim3(nblocks), dim3(kBT), &a, sizeof(a), &bs.ctl->loop, max_iters, s));
-    PB_TRY(cudaEventRecord(ev[2], s));
-    batch_out_kernel<<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, ncols, c0, g.inv, bs.S, out_old);
-    nl++;
-    PB_TRY(cudaGetLastError());
-    PB_TRY(cudaMemcpyAsync(sweeps_tile.data(), bs.sweeps, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, s));
-    if (max_iters)
-      PB_TRY(cudaMemcpyAsync(trace_tile.data(), bs.trace, sizeof(double) * static_cast<int64_t>(max_iters) * B,
-                             cudaMemcpyDeviceToHost, s));
-    PB_TRY(cudaStreamSynchronize(s));
+    const int Bp = PadWidth(B);
+    std::fill(trace_tile.begin(), trace_tile.end(), 0.0);
     float ms = 0;
-    cudaEventElapsedTime(&ms, ev[1], ev[2]);
+    cudaError_t e = SolveTile(g, bs, s, max_iters, epsilon, damping, ncols, c0, B, Bp, tele_old,
+                              out_old, sweeps_tile.data(), trace_tile.data(), &ms, &nl, err);
+    if (e != cudaSuccess) return e;
     sweep_total += ms;
-    int tile_loops = 0;
-    for (int c = 0; c < B; c++) tile_loops = std::max(tile_loops, sweeps_tile[c]);
-    nl += 2 * tile_loops;  // sweep + decide kernel per executed sweep
     for (int c = 0; c < B; c++) {
       if (sweeps_out) sweeps_out[c0 + c] = sweeps_tile[c];
       if (err_trace)
         for (int it = 0; it < max_iters; it++)
-          err_trace[static_cast<int64_t>(it) * ncols + c0 + c] = trace_tile[static_cast<int64_t>(it) * B + c];
+          err_trace[static_cast<int64_t>(it) * ncols + c0 + c] =
+              trace_tile[static_cast<int64_t>(it) * kMaxTile + c];
     }
   }
-  PB_TRY(cudaEventRecord(ev[3], s));
-  PB_TRY(cudaEventSynchronize(ev[3]));
+  PB_TRY(cudaEventRecord(t1, s));
+  PB_TRY(cudaEventSynchronize(t1));
   float tot = 0;
-  cudaEventElapsedTime(&tot, ev[0], ev[3]);
-  for (auto &e : ev) cudaEventDestroy(e);
+  cudaEventElapsedTime(&tot, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
   *ms_sweep = sweep_total;
   *ms_total = tot;
   *launches = nl;

@@ -11,34 +11,44 @@
 
 namespace prgpu {
 
-// Widest column tile one batched sweep processes (two columns per lane).
+// Column tile widths a batched sweep supports (floats per score-block row).
+// Widths are padded up to one of these; padding columns never iterate.
 constexpr int kMaxTile = 64;
+constexpr int kTileWidths[4] = {8, 16, 32, 64};
 
 struct BatchCtl {
   LoopCtl loop;               // done flag + sweep index (see loop_graph.h)
   unsigned tick2;             // stage-2 ticket of the grid reduction
-  int pad;
+  int compact;                // loop stopped so the survivors can be repacked
   unsigned long long active;  // bit c set while column c of the tile iterates
 };
 
 struct BatchScratch {
+  // Two score/base sets: a repack copies the surviving columns of one set
+  // into the other.  The two contrib buffers are shared by both sets.
   float *S = nullptr, *C[2] = {nullptr, nullptr}, *base = nullptr;
+  float *S2 = nullptr, *base2 = nullptr;
   double *part1 = nullptr, *part2 = nullptr, *trace = nullptr;
   unsigned *tick1 = nullptr;
   int32_t *sweeps = nullptr;
   float *seg_partial = nullptr;
   BatchCtl *ctl = nullptr;
-  int64_t cap_cells = 0, cap_part = 0, cap_trace = 0, cap_seg = 0;
-  int tile = 0;  // column tile width (0 = automatic)
-  LoopGraph loop;
+  int64_t cap_cells = 0, cap_cells2 = 0, cap_part = 0, cap_groups = 0, cap_trace = 0, cap_seg = 0;
+  // Column tile width: 0 = chosen by the autotuner (once per uploaded graph
+  // and column count), else one of kTileWidths.
+  int tile = 0;
+  int tuned_tile = 0;       // autotuner's choice for tuned_ncols
+  int tuned_ncols = 0;
+  const void *tuned_graph = nullptr;
+  LoopGraph loop[4];        // one cached sweep-loop graph per tile width
 };
 
 void FreeBatchScratch(BatchScratch *b);
 
 // Solves ncols personalized PageRank columns (teleport N x ncols, original
-// ids, device) into out (N x ncols, original ids, device), in tiles of up
-// to kMaxTile columns.  sweeps_out / err_trace are host arrays (nullable)
-// laid out as in pr_gpu_run.
+// ids, device; nullptr = every column uniform 1/N) into out (N x ncols,
+// original ids, device), one column tile at a time.  sweeps_out / err_trace
+// are host arrays (nullable) laid out as in pr_gpu_run.
 cudaError_t SolveBatched(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s,
                          int max_iters, double epsilon, float damping, int ncols,
                          const float *tele_old, float *out_old, int32_t *sweeps_out,

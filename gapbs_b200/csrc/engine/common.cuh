@@ -78,6 +78,27 @@ __device__ __forceinline__ float ld_gather(const float *p, uint64_t pol) {
   return r;
 }
 
+__device__ __forceinline__ float4 ld_gather_v4(const float4 *p, uint64_t pol) {
+  float4 r;
+  asm("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+      : "l"(p), "l"(pol));
+  return r;
+}
+
+__device__ __forceinline__ float4 ld_score_v4(const float4 *p, uint64_t pol) {
+  float4 r;
+  asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+               : "l"(p), "l"(pol));
+  return r;
+}
+
+__device__ __forceinline__ void st_hint_v4(float4 *p, float4 v, uint64_t pol) {
+  asm volatile("st.global.L1::no_allocate.L2::cache_hint.v4.f32 [%0], {%1,%2,%3,%4}, %5;"
+               :: "l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "l"(pol) : "memory");
+}
+
 __device__ __forceinline__ void st_hint_f32(float *p, float v, uint64_t pol) {
   asm volatile("st.global.L1::no_allocate.L2::cache_hint.f32 [%0], %1, %2;"
                :: "l"(p), "f"(v), "l"(pol) : "memory");

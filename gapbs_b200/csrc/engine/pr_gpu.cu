@@ -556,6 +556,20 @@ int pr_gpu_adjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping,
   return rc;
 }
 
+int pr_gpu_set_batch_tile(pr_gpu_t *h, int width) {
+  if (!h) return PR_GPU_EINVAL;
+  if (width != 0 && width != 8 && width != 16 && width != 32 && width != 64)
+    return SetErr(h, PR_GPU_EINVAL, "batch tile width must be 0, 8, 16, 32 or 64");
+  h->bsc.tile = width;
+  return PR_GPU_OK;
+}
+
+int pr_gpu_get_batch_tile(const pr_gpu_t *h, int *width) {
+  if (!h || !width) return PR_GPU_EINVAL;
+  *width = h->bsc.tile ? h->bsc.tile : h->bsc.tuned_tile;
+  return PR_GPU_OK;
+}
+
 int pr_gpu_set_stream(pr_gpu_t *h, void *stream) {
   if (!h) return PR_GPU_EINVAL;
   PR_CHECK(h, cudaSetDevice(h->device));

@@ -170,6 +170,15 @@ class PageRankEngine:
         self._check(rc, "pr_gpu_adjoint_device")
         return int(sw[0])
 
+    def set_batch_tile(self, width: int):
+        """Column tile width of batched solves (8/16/32/64), 0 = autotuned."""
+        self._check(self._lib.pr_gpu_set_batch_tile(self._h, int(width)), "pr_gpu_set_batch_tile")
+
+    def batch_tile(self) -> int:
+        w = ctypes.c_int()
+        self._check(self._lib.pr_gpu_get_batch_tile(self._h, byref(w)), "pr_gpu_get_batch_tile")
+        return w.value
+
     def set_stream(self, stream_handle: Optional[int]):
         """Issue work on a caller stream (raw cudaStream_t), None = own stream."""
         self._check(self._lib.pr_gpu_set_stream(self._h, stream_handle), "pr_gpu_set_stream")

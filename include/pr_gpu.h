@@ -114,6 +114,14 @@ int pr_gpu_adjoint_device(pr_gpu_t *h, int max_iters, double epsilon,
                           const float *scores_dev, float *grad_teleport_dev,
                           float *grad_edge_w_dev, int32_t *sweeps_out);
 
+/* Column tile width of batched (ncols > 1) solves: 8, 16, 32 or 64 score
+ * columns per block row, or 0 (the default) to let the engine's autotuner
+ * time each width on the first batched solve of a graph and column count
+ * and keep the fastest.  pr_gpu_get_batch_tile reports the width in use
+ * (0 before any batched solve under the autotuner). */
+int pr_gpu_set_batch_tile(pr_gpu_t *h, int width);
+int pr_gpu_get_batch_tile(const pr_gpu_t *h, int *width);
+
 /* Makes the handle issue its work on `stream` (a cudaStream_t of the
  * handle's device, e.g. the caller's framework stream) instead of its own;
  * NULL restores the handle's own stream.  The handle does not take
