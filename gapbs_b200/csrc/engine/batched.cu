@@ -36,6 +36,7 @@ namespace {
 constexpr int kBT = 256;       // threads per block
 constexpr int kBW = kBT / 32;  // warps per block
 constexpr int kUnroll = 4;     // gather instructions in flight per lane
+constexpr int64_t kL1GatherBytes = 96 * 1024;  // L1 budget for hub rows per SM
 
 struct BatchArgs {
   int32_t n;
@@ -65,6 +66,9 @@ struct BatchArgs {
   int32_t *sweeps;
   int32_t nblocks;
   int32_t stop_at;  // stop for a repack once at most this many columns iterate
+  int32_t zero_final_sweep;  // first sweep that may skip rows without in-neighbours
+  int32_t l1_rows;  // rows [0, l1_rows) (the hubs) are gathered through L1; the
+                    // rest bypass it so they cannot evict the hubs
   double epsilon;
 };
 
@@ -116,8 +120,12 @@ __device__ __forceinline__ float4 row_accumulate(const BatchArgs &a, const float
         const int v = __shfl_sync(0xffffffffu, idx, kk & 31);
         wk[q] = W ? __shfl_sync(0xffffffffu, w, kk & 31) : 1.f;
         x[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (gather && kk < cnt)
-          x[q] = ld_gather_v4(reinterpret_cast<const float4 *>(Cin + static_cast<int64_t>(v) * Bp) + gl, pg);
+        if (gather && kk < cnt) {
+          // element offset < 2^32 (n * 64 fits while n < 2^26)
+          const float4 *src = reinterpret_cast<const float4 *>(
+              Cin + (static_cast<uint32_t>(v) * static_cast<uint32_t>(Bp) + 4u * gl));
+          x[q] = v < a.l1_rows ? ld_gather_v4(src, pg) : ld_gather_v4_cold(src, pg);
+        }
       }
 #pragma unroll
       for (int q = 0; q < kUnroll; q++) {
@@ -155,12 +163,14 @@ __device__ __forceinline__ void finish4(const BatchArgs &a, float *Cout, int u, 
                                         float den, double err[4], uint64_t ps, uint64_t pl) {
   const int64_t i = static_cast<int64_t>(u) * a.Bp + 4 * gl;
   float nw[4], cv[4];
+  // one division per row; contrib = new * (1 / S_v) is within an ulp of new / S_v
+  const float inv = __frcp_rn(den);
 #pragma unroll
   for (int c = 0; c < 4; c++) {
     const float o = comp(old, c);
     const bool act = (active4 >> c) & 1u;
     nw[c] = act ? __fadd_rn(comp(bs, c), __fmul_rn(a.damping, comp(sum, c))) : o;
-    cv[c] = __fdiv_rn(nw[c], den);
+    cv[c] = __fmul_rn(nw[c], inv);
     if (act) err[c] += static_cast<double>(fabsf(__fsub_rn(nw[c], o)));
   }
   st_hint_v4(reinterpret_cast<float4 *>(a.S + i), make_float4(nw[0], nw[1], nw[2], nw[3]), ps);
@@ -242,7 +252,12 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
   // ---- every other row: one warp per row, interleaved across the grid
   const int gw = blockIdx.x * kBW + wid;
   const int nw = gridDim.x * kBW;
-  for (int u = a.hub_rows + gw; u < a.n; u += nw) {
+  // Rows without in-neighbours hold new = base from the first sweep on; their
+  // contrib is final once both ping-pong buffers hold it (after the second
+  // sweep; an undirected graph never gathers it at all).  Later sweeps skip
+  // them: their scores cannot change and their L1 change is exactly zero.
+  const int row_end = (it >= a.zero_final_sweep) ? a.zero_start : a.n;
+  for (int u = a.hub_rows + gw; u < row_end; u += nw) {
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     if (u < a.zero_start)
       acc = row_accumulate<L, W>(a, Cin, a.rowoff[u], a.rowoff[u + 1], lane, gather, ps, pg);
@@ -370,15 +385,16 @@ __global__ void batch_init_kernel(int32_t n, int B, int Bp, int K, int c0,
   C[i] = __fdiv_rn(t, denom);
 }
 
-// Writes tile columns j < B (caller column map.c[j]) back in original ids.
-__global__ void batch_out_kernel(int32_t n, int B, int Bp, int K, ColMap map,
+// Writes tile columns src.c[j] (j < B) to caller columns dst.c[j], in
+// original vertex ids.
+__global__ void batch_out_kernel(int32_t n, int B, int Bp, int K, ColMap src, ColMap dst,
                                  const int32_t *__restrict__ inv, const float *__restrict__ S,
                                  float *out_old) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= static_cast<int64_t>(n) * B) return;
   const int64_t v = i / B;
   const int j = static_cast<int>(i - v * B);
-  out_old[v * K + map.c[j]] = S[static_cast<int64_t>(inv[v]) * Bp + j];
+  out_old[v * K + dst.c[j]] = S[static_cast<int64_t>(inv[v]) * Bp + src.c[j]];
 }
 
 template <typename T>
@@ -556,6 +572,12 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
     a.sweeps = bs.sweeps;
     a.nblocks = nblocks;
     a.stop_at = tile_bp > 8 ? tile_bp / 2 : 0;
+    // Directed graphs gather the contribs of rows without in-neighbours, so
+    // both ping-pong buffers must hold them in this phase's layout: those rows
+    // are processed in the phase's first two sweeps.  Undirected graphs never
+    // gather them (no in-neighbour means no out-neighbour).
+    a.zero_final_sweep = g.directed ? loops + 2 : 1;
+    a.l1_rows = static_cast<int32_t>(std::min<int64_t>(n, kL1GatherBytes / (4 * tile_bp)));
     a.epsilon = epsilon;
     PB_TRY(cudaEventRecord(e0, s));
     PB_TRY(bs.loop[WidthIndex(tile_bp)].Launch(fn, dim3(nblocks), dim3(kBT), &a, sizeof(a),
@@ -568,15 +590,27 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
       PB_TRY(cudaMemcpyAsync(tr.data(), bs.trace,
                              sizeof(double) * static_cast<int64_t>(max_iters) * tile_bp,
                              cudaMemcpyDeviceToHost, s));
-    // every column of this phase leaves its scores in the caller's block; a
-    // column still iterating is overwritten by a later phase
-    if (out_old) {
-      batch_out_kernel<<<static_cast<unsigned>((n * nact + T - 1) / T), T, 0, s>>>(
-          static_cast<int32_t>(n), nact, tile_bp, K, map, g.inv, S, out_old);
-      PB_TRY(cudaGetLastError());
-      *launches += 1;
-    }
     PB_TRY(cudaStreamSynchronize(s));
+    // write back the columns that are final: those that retired in this
+    // phase, or all of them when the tile is done
+    const bool last_phase = !ctl.compact || ctl.loop.loops >= max_iters;
+    if (out_old) {
+      ColMap fin_src, fin_dst;
+      int nfin = 0;
+      for (int j = 0; j < nact; j++)
+        if (last_phase || !((ctl.active >> j) & 1ull)) {
+          fin_src.c[nfin] = j;
+          fin_dst.c[nfin] = map.c[j];
+          nfin++;
+        }
+      for (int j = nfin; j < kMaxTile; j++) fin_src.c[j] = fin_dst.c[j] = 0;
+      if (nfin) {
+        batch_out_kernel<<<static_cast<unsigned>((n * nfin + T - 1) / T), T, 0, s>>>(
+            static_cast<int32_t>(n), nfin, tile_bp, K, fin_src, fin_dst, g.inv, S, out_old);
+        PB_TRY(cudaGetLastError());
+        *launches += 1;
+      }
+    }
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     *sweep_ms += ms;

@@ -78,9 +78,25 @@ __device__ __forceinline__ float ld_gather(const float *p, uint64_t pol) {
   return r;
 }
 
+// Gather that does not allocate in L1 (cold rows must not evict the hubs).
+__device__ __forceinline__ float ld_gather_cold(const float *p, uint64_t pol) {
+  float r;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;"
+               : "=f"(r) : "l"(p), "l"(pol));
+  return r;
+}
+
 __device__ __forceinline__ float4 ld_gather_v4(const float4 *p, uint64_t pol) {
   float4 r;
   asm("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+      : "l"(p), "l"(pol));
+  return r;
+}
+
+__device__ __forceinline__ float4 ld_gather_v4_cold(const float4 *p, uint64_t pol) {
+  float4 r;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
       : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
       : "l"(p), "l"(pol));
   return r;

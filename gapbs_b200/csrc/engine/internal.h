@@ -139,8 +139,16 @@ struct PullArgs {
   double *trace;
   SweepCtl *ctl;
   int32_t nblocks;
+  // Vertices [0, l1_rows) -- the highest-degree ones after renumbering -- are
+  // gathered through L1; the rest bypass L1 so they cannot evict them.
+  int32_t l1_rows;
+  // From this sweep on, rows without in-neighbours are final and skipped.
+  int32_t zero_final_sweep;
   double epsilon;
 };
+
+// L1 budget per SM for hub contribs of a single-column sweep.
+constexpr int kL1HubBytes = 128 * 1024;
 
 // Launchers (kernels.cu / prep.cu).
 cudaError_t BuildDeviceGraph(DeviceGraph *g, int64_t n, int64_t m,

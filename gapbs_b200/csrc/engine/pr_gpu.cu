@@ -258,6 +258,8 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
   a.trace = sc.trace;
   a.ctl = sc.ctl;
   a.nblocks = nblocks;
+  a.l1_rows = static_cast<int32_t>(std::min<int64_t>(g.n, prgpu::kL1HubBytes / 4));
+  a.zero_final_sweep = g.directed ? 2 : 1;
   a.epsilon = epsilon;
   a.c0 = sc.contrib[0];
   a.c1 = sc.contrib[1];
@@ -351,6 +353,8 @@ int SolveAdjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping, cons
   a.trace = sc.trace;
   a.ctl = sc.ctl;
   a.nblocks = nblocks;
+  a.l1_rows = static_cast<int32_t>(std::min<int64_t>(g.n, prgpu::kL1HubBytes / 4));
+  a.zero_final_sweep = 1;  // bins path: undirected only
   a.epsilon = epsilon * wnorm;
   a.c0 = sc.contrib[0];
   a.c1 = sc.contrib[1];

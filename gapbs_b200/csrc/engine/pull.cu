@@ -33,19 +33,23 @@ __device__ __forceinline__ float pr_update(float base, float d, float sum) {
   return __fadd_rn(base, __fmul_rn(d, sum));
 }
 
+__device__ __forceinline__ float ld_contrib(const float *cin, int v, int l1_rows, uint64_t pg) {
+  return v < l1_rows ? ld_gather(cin + v, pg) : ld_gather_cold(cin + v, pg);
+}
+
 template <bool W>
 __device__ __forceinline__ float gather_chunk(float acc, const int4 q, const float4 w,
                                               int b, int s, int e, const float *cin,
-                                              uint64_t pg) {
+                                              int l1_rows, uint64_t pg) {
   const bool i0 = (b >= s) & (b < e);
   const bool i1 = (b + 1 >= s) & (b + 1 < e);
   const bool i2 = (b + 2 >= s) & (b + 2 < e);
   const bool i3 = (b + 3 >= s) & (b + 3 < e);
   float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-  if (i0) v0 = ld_gather(cin + q.x, pg);
-  if (i1) v1 = ld_gather(cin + q.y, pg);
-  if (i2) v2 = ld_gather(cin + q.z, pg);
-  if (i3) v3 = ld_gather(cin + q.w, pg);
+  if (i0) v0 = ld_contrib(cin, q.x, l1_rows, pg);
+  if (i1) v1 = ld_contrib(cin, q.y, l1_rows, pg);
+  if (i2) v2 = ld_contrib(cin, q.z, l1_rows, pg);
+  if (i3) v3 = ld_contrib(cin, q.w, l1_rows, pg);
   if (W) {
     if (i0) acc = __fmaf_rn(w.x, v0, acc);
     if (i1) acc = __fmaf_rn(w.y, v1, acc);
@@ -85,10 +89,10 @@ __device__ __forceinline__ float lane_partial(const PullArgs &a, const float *ci
       w2 = ld_stream_v4f(w4 + c + 2 * G, ps);
       w3 = ld_stream_v4f(w4 + c + 3 * G, ps);
     }
-    acc = gather_chunk<W>(acc, q0, w0, c << 2, s, e, cin, pg);
-    acc = gather_chunk<W>(acc, q1, w1, (c + G) << 2, s, e, cin, pg);
-    acc = gather_chunk<W>(acc, q2, w2, (c + 2 * G) << 2, s, e, cin, pg);
-    acc = gather_chunk<W>(acc, q3, w3, (c + 3 * G) << 2, s, e, cin, pg);
+    acc = gather_chunk<W>(acc, q0, w0, c << 2, s, e, cin, a.l1_rows, pg);
+    acc = gather_chunk<W>(acc, q1, w1, (c + G) << 2, s, e, cin, a.l1_rows, pg);
+    acc = gather_chunk<W>(acc, q2, w2, (c + 2 * G) << 2, s, e, cin, a.l1_rows, pg);
+    acc = gather_chunk<W>(acc, q3, w3, (c + 3 * G) << 2, s, e, cin, a.l1_rows, pg);
   }
   if (c < c1) {
     // up to three remaining chunks, loads predicated on the row's last chunk
@@ -102,9 +106,9 @@ __device__ __forceinline__ float lane_partial(const PullArgs &a, const float *ci
       if (h1) w1 = ld_stream_v4f(w4 + c + G, ps);
       if (h2) w2 = ld_stream_v4f(w4 + c + 2 * G, ps);
     }
-    acc = gather_chunk<W>(acc, q0, w0, c << 2, s, e, cin, pg);
-    if (h1) acc = gather_chunk<W>(acc, q1, w1, (c + G) << 2, s, e, cin, pg);
-    if (h2) acc = gather_chunk<W>(acc, q2, w2, (c + 2 * G) << 2, s, e, cin, pg);
+    acc = gather_chunk<W>(acc, q0, w0, c << 2, s, e, cin, a.l1_rows, pg);
+    if (h1) acc = gather_chunk<W>(acc, q1, w1, (c + G) << 2, s, e, cin, a.l1_rows, pg);
+    if (h2) acc = gather_chunk<W>(acc, q2, w2, (c + 2 * G) << 2, s, e, cin, a.l1_rows, pg);
   }
   return acc;
 }
@@ -295,7 +299,9 @@ pull_sweep_kernel(const PullArgs a) {
   const int lane32 = threadIdx.x & 31;
   const int gw = blockIdx.x * (kSweepThreads / 32) + (threadIdx.x >> 5);
   const int nw = gridDim.x * (kSweepThreads / 32);
-  const int ntasks = a.task_start[kNumBins];
+  // rows without in-neighbours (the last bin) are final after their first
+  // sweep (their second for a directed graph, whose contribs they supply)
+  const int ntasks = (it >= a.zero_final_sweep) ? a.task_start[kBinZero] : a.task_start[kNumBins];
   for (int t = gw; t < ntasks; t += nw) {
     int bin = 1;
 #pragma unroll
