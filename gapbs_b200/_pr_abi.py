@@ -18,7 +18,7 @@ SYMBOLS = (
     "pr_gpu_create", "pr_gpu_upload", "pr_gpu_run", "pr_gpu_run_device",
     "pr_gpu_adjoint", "pr_gpu_adjoint_device", "pr_gpu_set_stream",
     "pr_gpu_set_batch_tile", "pr_gpu_get_batch_tile", "pr_gpu_last_timing",
-    "pr_gpu_graph_info", "pr_gpu_run_noalloc", "pr_gpu_destroy", "pr_gpu_last_error",
+    "pr_gpu_graph_info", "pr_gpu_measure_gather_rate", "pr_gpu_run_noalloc", "pr_gpu_destroy", "pr_gpu_last_error",
 )
 
 
@@ -46,6 +46,8 @@ def declare(lib):
     lib.pr_gpu_graph_info.argtypes = [P, POINTER(c_int64), POINTER(c_int64), POINTER(c_int64),
                                       POINTER(c_int64), c_int]
     lib.pr_gpu_graph_info.restype = c_int
+    lib.pr_gpu_measure_gather_rate.argtypes = [c_int, c_int64, POINTER(c_double)]
+    lib.pr_gpu_measure_gather_rate.restype = c_int
     lib.pr_gpu_run_noalloc.argtypes = [c_int, c_int64, c_int64, P, P, P, c_int, c_double, c_float,
                                        P, P, P, P, c_char_p, c_size_t]
     lib.pr_gpu_run_noalloc.restype = c_int

@@ -211,6 +211,18 @@ def engine_for(g: Graph, device: int = 0) -> PageRankEngine:
     return eng
 
 
+def measure_gather_rate(array_bytes: int, device: int = 0) -> float:
+    """Random 4-byte gathers per second that bypass L1, from an array of
+    array_bytes (see pr_gpu_measure_gather_rate): the ceiling of the sweep
+    kernels' gathers when the array fits in L2."""
+    lib = pr_lib()
+    out = c_double()
+    rc = lib.pr_gpu_measure_gather_rate(int(device), int(array_bytes), byref(out))
+    if rc != 0:
+        raise PageRankError(rc, "pr_gpu_measure_gather_rate failed")
+    return out.value
+
+
 def print_step(step: int, value: float) -> None:
     """The reference's -l line (src/util.h:37-46): '%5s%23.5lf'."""
     print(f"{step:>5d}{value:23.5f}")

@@ -138,6 +138,16 @@ int pr_gpu_last_timing(const pr_gpu_t *h, double *sweep_ms, double *total_ms,
 int pr_gpu_graph_info(const pr_gpu_t *h, int64_t *n, int64_t *m,
                       int64_t *max_degree, int64_t *bin_rows, int nbins);
 
+/* Diagnostic: the random-gather ceiling of this GPU.  Times independent
+ * 4-byte loads at hashed addresses inside a device array of array_bytes
+ * (rounded down to a power of two; far larger than L1), and returns the loads
+ * completed per second.  A pull sweep issues one such load per edge, so with
+ * an array that fits in L2 this is the rate that bounds the sweep kernels
+ * when their gathers miss L1 (each costs a 32-byte sector request between
+ * the SM and L2).  Allocates and frees its own buffers.  No counterpart in
+ * the reference. */
+int pr_gpu_measure_gather_rate(int device, int64_t array_bytes, double *gathers_per_s);
+
 /* Upper limits of pr_gpu_run_noalloc (sizes of its fixed scratch area). */
 #define PR_GPU_NOALLOC_MAX_VERTICES (1 << 20)
 #define PR_GPU_NOALLOC_MAX_ITERS 1024
