@@ -19,7 +19,15 @@
 // sweep): a persistent grid (SMs x resident blocks) first takes the hub-row
 // segments block-cooperatively (the row's last segment block sums the
 // segment partials in segment order), then every warp takes whole rows,
-// interleaved across the grid.
+// interleaved across the grid, and finally the short rows (fewer in-entries
+// than two rounds of a warp's gathers) go one row per lane group, 32/L rows
+// per warp at once, so the per-row work (offsets, old score, update, stores)
+// of the many short rows runs in parallel instead of one row at a time.
+//
+// L2 policy: the first hot_rows rows of the block (the highest in-degree
+// vertices, gathered most often) are written and gathered evict-last; the
+// other rows evict-first, so the streams of cold rows do not push the hub
+// rows out of L2.  The first l1_rows rows are also gathered through L1.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,6 +45,11 @@ constexpr int kBT = 256;       // threads per block
 constexpr int kBW = kBT / 32;  // warps per block
 constexpr int kUnroll = 4;     // gather instructions in flight per lane
 constexpr int64_t kL1GatherBytes = 96 * 1024;  // L1 budget for hub rows per SM
+#ifndef GAPBS_BATCH_L2_HOT_MB
+#define GAPBS_BATCH_L2_HOT_MB 80
+#endif
+// L2 budget for the evict-last hub rows of the contrib block.
+constexpr int64_t kL2HotBytes = static_cast<int64_t>(GAPBS_BATCH_L2_HOT_MB) << 20;
 
 struct BatchArgs {
   int32_t n;
@@ -47,6 +60,7 @@ struct BatchArgs {
   const int32_t *__restrict__ odeg;
   const float *__restrict__ rsum;
   const float *__restrict__ base;
+  const uint8_t *__restrict__ tflag;  // row has a nonzero base entry
   float damping;
   float *S;
   float *C0;  // contrib ping-pong: sweep k gathers C[k & 1], writes C[(k + 1) & 1]
@@ -69,6 +83,8 @@ struct BatchArgs {
   int32_t zero_final_sweep;  // first sweep that may skip rows without in-neighbours
   int32_t l1_rows;  // rows [0, l1_rows) (the hubs) are gathered through L1; the
                     // rest bypass it so they cannot evict the hubs
+  int32_t hot_rows;     // rows [0, hot_rows) are kept in L2 (evict-last)
+  int32_t short_start;  // rows [short_start, n) go one row per lane group
   double epsilon;
 };
 
@@ -88,6 +104,16 @@ __device__ __forceinline__ float4 f4add(float4 a, float4 b) {
   return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
 }
 
+// Loads columns 4*gl .. 4*gl+3 of contrib row v with the row's cache policy.
+__device__ __forceinline__ float4 gather_row4(const BatchArgs &a, const float *Cin, int v, int gl,
+                                              uint64_t ps, uint64_t pg) {
+  // element offset < 2^32 (n * 64 fits while n < 2^26)
+  const float4 *src = reinterpret_cast<const float4 *>(
+      Cin + (static_cast<uint32_t>(v) * static_cast<uint32_t>(a.Bp) + 4u * gl));
+  const uint64_t pol = v < a.hot_rows ? pg : ps;
+  return v < a.l1_rows ? ld_gather_v4(src, pol) : ld_gather_v4_cold(src, pol);
+}
+
 // Sum over entries [s, e) of w_e * Cin[v_e, 4*gl .. 4*gl+3], where lane group
 // grp = lane / L takes every (32/L)-th entry; the caller reduces across
 // groups.  Indices (and weights) are loaded 32 at a time and broadcast.
@@ -98,7 +124,6 @@ __device__ __forceinline__ float4 row_accumulate(const BatchArgs &a, const float
                                                  float w_first = 0.f) {
   constexpr int NPW = 32 / L;
   const int grp = lane / L, gl = lane % L;
-  const int Bp = 4 * L;
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   for (int j0 = s; j0 < e; j0 += 32) {
     const int cnt = min(32, e - j0);
@@ -120,12 +145,7 @@ __device__ __forceinline__ float4 row_accumulate(const BatchArgs &a, const float
         const int v = __shfl_sync(0xffffffffu, idx, kk & 31);
         wk[q] = W ? __shfl_sync(0xffffffffu, w, kk & 31) : 1.f;
         x[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (gather && kk < cnt) {
-          // element offset < 2^32 (n * 64 fits while n < 2^26)
-          const float4 *src = reinterpret_cast<const float4 *>(
-              Cin + (static_cast<uint32_t>(v) * static_cast<uint32_t>(Bp) + 4u * gl));
-          x[q] = v < a.l1_rows ? ld_gather_v4(src, pg) : ld_gather_v4_cold(src, pg);
-        }
+        if (gather && kk < cnt) x[q] = gather_row4(a, Cin, v, gl, ps, pg);
       }
 #pragma unroll
       for (int q = 0; q < kUnroll; q++) {
@@ -147,6 +167,66 @@ __device__ __forceinline__ float4 row_accumulate(const BatchArgs &a, const float
     acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
     acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
     acc.w += __shfl_xor_sync(0xffffffffu, acc.w, o);
+  }
+  return acc;
+}
+
+// Short rows: lane group grp = lane / L owns one row (entries [s, s + len),
+// len may differ between groups) and sums w_e * Cin[v_e, 4*gl .. 4*gl+3]
+// over it, kUnroll gathers in flight per group.  Each lane loads CH / L of
+// every CH consecutive indices of its group's row; the loop runs to the
+// longest row of the warp (warp-uniform trip count, shuffles stay converged).
+template <int L, bool W>
+__device__ __forceinline__ float4 group_accumulate(const BatchArgs &a, const float *Cin, int s,
+                                                   int len, int lane, bool gather, uint64_t ps,
+                                                   uint64_t pg) {
+  constexpr int CH = L > kUnroll ? L : kUnroll;
+  constexpr int R = CH / L;
+  const int grp = lane / L, gl = lane % L;
+  int maxlen = len;
+#pragma unroll
+  for (int o = L; o < 32; o <<= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, o));
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int j0 = 0; j0 < maxlen; j0 += CH) {
+    int idx[R];
+    float w[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int j = j0 + r * L + gl;
+      idx[r] = 0;
+      w[r] = 0.f;
+      if (j < len) {
+        idx[r] = ld_stream_s32(a.col + s + j, ps);
+        if (W) w[r] = ld_stream_f32(a.win + s + j, ps);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < CH; k += kUnroll) {
+      if (j0 + k < maxlen) {  // warp-uniform
+        float4 x[kUnroll];
+        float wk[kUnroll];
+#pragma unroll
+        for (int q = 0; q < kUnroll; q++) {
+          const int kk = k + q;
+          const int srcl = grp * L + (kk % L);
+          const int v = __shfl_sync(0xffffffffu, idx[kk / L], srcl);
+          wk[q] = W ? __shfl_sync(0xffffffffu, w[kk / L], srcl) : 1.f;
+          x[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (gather && j0 + kk < len) x[q] = gather_row4(a, Cin, v, gl, ps, pg);
+        }
+#pragma unroll
+        for (int q = 0; q < kUnroll; q++) {
+          if (W) {
+            acc.x = __fmaf_rn(wk[q], x[q].x, acc.x);
+            acc.y = __fmaf_rn(wk[q], x[q].y, acc.y);
+            acc.z = __fmaf_rn(wk[q], x[q].z, acc.z);
+            acc.w = __fmaf_rn(wk[q], x[q].w, acc.w);
+          } else {
+            acc = f4add(acc, x[q]);
+          }
+        }
+      }
+    }
   }
   return acc;
 }
@@ -239,7 +319,8 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
           sum = __fadd_rn(sum, __ldcg(a.seg_partial + static_cast<int64_t>(first + k) * Bp + c));
         const int64_t i = static_cast<int64_t>(u) * Bp + c;
         const float old = ld_score(a.S + i, ps);
-        const float nw = __fadd_rn(a.base[i], __fmul_rn(a.damping, sum));
+        const float b0 = a.tflag[u] ? a.base[i] : 0.f;
+        const float nw = __fadd_rn(b0, __fmul_rn(a.damping, sum));
         st_hint_f32(a.S + i, nw, ps);
         st_hint_f32(Cout + i, __fdiv_rn(nw, bdenom<W, DIR>(a, u)), pg);
         scol[c] += static_cast<double>(fabsf(__fsub_rn(nw, old)));
@@ -257,16 +338,56 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
   // sweep; an undirected graph never gathers it at all).  Later sweeps skip
   // them: their scores cannot change and their L1 change is exactly zero.
   const int row_end = (it >= a.zero_final_sweep) ? a.zero_start : a.n;
-  for (int u = a.hub_rows + gw; u < row_end; u += nw) {
+  const int warp_end = min(max(a.short_start, a.hub_rows), row_end);
+  for (int u = a.hub_rows + gw; u < warp_end; u += nw) {
+    float4 old = make_float4(0.f, 0.f, 0.f, 0.f), bs = old;
+    const int64_t i = static_cast<int64_t>(u) * Bp + 4 * gl;
+    int fl = 0;
+    if (lane < L && gather) {  // issued before the gathers, consumed after
+      old = ld_score_v4(reinterpret_cast<const float4 *>(a.S + i), ps);
+      fl = __ldg(a.tflag + u);
+    }
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     if (u < a.zero_start)
       acc = row_accumulate<L, W>(a, Cin, a.rowoff[u], a.rowoff[u + 1], lane, gather, ps, pg);
     if (lane < L && gather) {
-      const int64_t i = static_cast<int64_t>(u) * Bp + 4 * gl;
-      const float4 old = ld_score_v4(reinterpret_cast<const float4 *>(a.S + i), ps);
-      const float4 bs = *reinterpret_cast<const float4 *>(a.base + i);
-      finish4<W, DIR>(a, Cout, u, gl, active4, acc, old, bs, bdenom<W, DIR>(a, u), err, ps, pg);
+      if (fl) bs = ld_stream_v4f(reinterpret_cast<const float4 *>(a.base + i), ps);
+      finish4<W, DIR>(a, Cout, u, gl, active4, acc, old, bs, bdenom<W, DIR>(a, u), err, ps,
+                      u < a.hot_rows ? pg : ps);
     }
+  }
+  {
+    constexpr int NPW = 32 / L;
+    const int grp = lane / L;
+    const int sbeg = max(warp_end, a.hub_rows);
+    for (int u0 = sbeg + gw * NPW; u0 < row_end; u0 += nw * NPW) {
+      const int u = u0 + grp;
+      const bool valid = u < row_end;
+      int s = 0, len = 0;
+      if (valid && u < a.zero_start) {
+        s = a.rowoff[u];
+        len = a.rowoff[u + 1] - s;
+      }
+      float4 old = make_float4(0.f, 0.f, 0.f, 0.f), bs = old;
+      const int64_t i = static_cast<int64_t>(u) * Bp + 4 * gl;
+      int fl = 0;
+      if (valid && gather) {
+        old = ld_score_v4(reinterpret_cast<const float4 *>(a.S + i), ps);
+        fl = __ldg(a.tflag + u);
+      }
+      const float4 acc = group_accumulate<L, W>(a, Cin, s, len, lane, gather, ps, pg);
+      if (valid && gather) {
+        if (fl) bs = ld_stream_v4f(reinterpret_cast<const float4 *>(a.base + i), ps);
+        finish4<W, DIR>(a, Cout, u, gl, active4, acc, old, bs, bdenom<W, DIR>(a, u), err, ps,
+                        u < a.hot_rows ? pg : ps);
+      }
+    }
+  }
+  // lane groups hold partial errors of the same columns: combine them
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+#pragma unroll
+    for (int o = L; o < 32; o <<= 1) err[c] += __shfl_xor_sync(0xffffffffu, err[c], o);
   }
 
   // ---- per-column block partial, then two-stage grid reduction per column
@@ -336,65 +457,192 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
   }
 }
 
+// The per-tile copy kernels below run on a grid of kCopyBlocksPerSM blocks
+// per SM and stride over their cells, four independent cells in flight per
+// thread: launching one short-lived thread per cell (hundreds of millions of
+// them for a 64-column tile) would be bound by block launch, not by HBM.
+// Cells are (row, column) with 2^lb column slots per row; the grid's thread
+// count is a multiple of 2^lb, so a thread keeps one column for all its
+// cells and reads its entry of the column tables (kernel parameters) once:
+// 32 different parameter-array entries per warp instruction would be
+// serialised by the constant cache on every cell.
+constexpr int kCopyBlocksPerSM = 8;
+constexpr int kCopyThreads = 256;
+
 // Copies the surviving columns map.c[j] (j < nact) of a width-Bo tile into
-// columns j of a width-Bn tile (padding columns zero).
-__global__ void batch_repack_kernel(int32_t n, int Bo, int Bn, int nact, ColMap map,
-                                    const float *__restrict__ So, const float *__restrict__ bo,
-                                    const float *__restrict__ Co, float *Sn, float *bn, float *Cn) {
-  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= static_cast<int64_t>(n) * Bn) return;
-  const int64_t u = i / Bn;
-  const int j = static_cast<int>(i - u * Bn);
-  if (j >= nact) {
-    Sn[i] = 0.f;
-    bn[i] = 0.f;
-    Cn[i] = 0.f;
-    return;
+// columns j of a width-2^lbn tile (padding columns zero); base is copied on
+// flagged rows only.
+__global__ void __launch_bounds__(kCopyThreads)
+    batch_repack_kernel(int32_t n, int Bo, int lbn, int nact, ColMap map,
+                        const uint8_t *__restrict__ tflag, const float *__restrict__ So,
+                        const float *__restrict__ bo, const float *__restrict__ Co,
+                        float *__restrict__ Sn, float *__restrict__ bn, float *__restrict__ Cn) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int j = static_cast<int>(t & ((1 << lbn) - 1));
+  const int64_t ustride = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> lbn;
+  const bool real = j < nact;
+  const int sc = real ? map.c[j] : 0;
+  for (int64_t u0 = t >> lbn; u0 < n; u0 += 4 * ustride) {
+    float sv[4], cv[4], bv[4];
+    bool fl[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int64_t u = u0 + r * ustride;
+      sv[r] = cv[r] = bv[r] = 0.f;
+      fl[r] = false;
+      if (u < n) {
+        fl[r] = tflag[u] != 0;
+        if (real) {
+          const int64_t src = u * Bo + sc;
+          sv[r] = So[src];
+          cv[r] = Co[src];
+          if (fl[r]) bv[r] = bo[src];
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int64_t u = u0 + r * ustride;
+      if (u < n) {
+        const int64_t i = (u << lbn) + j;
+        Sn[i] = sv[r];
+        Cn[i] = cv[r];
+        if (fl[r]) bn[i] = bv[r];
+      }
+    }
   }
-  const int64_t src = u * Bo + map.c[j];
-  Sn[i] = So[src];
-  bn[i] = bo[src];
-  Cn[i] = Co[src];
 }
 
-// Tile init: S = t, base = (1-d) t, C = t / S_v for the tile's real columns;
-// padding columns are zero.
+// Tile init, one thread per four columns of a row: S = t, C = t / S_v,
+// base = (1-d) t (written only on rows with a nonzero teleport entry, which
+// tflag marks); padding columns are zero.  Cell i is row u = i >> lq,
+// columns 4 * (i & (Bp/4 - 1)) ..; a row's cells are consecutive lanes of
+// one warp (Bp/4 <= 16), and whole warps stride together so the row-wide
+// ballot always has all 32 lanes.
 template <bool W, bool DIR>
-__global__ void batch_init_kernel(int32_t n, int B, int Bp, int K, int c0,
-                                  const int32_t *__restrict__ perm,
-                                  const int32_t *__restrict__ rowoff, const int32_t *__restrict__ odeg,
-                                  const float *__restrict__ rsum, const float *__restrict__ tele_old,
-                                  float uniform, float one_minus_d, float *S, float *C, float *base) {
-  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= static_cast<int64_t>(n) * Bp) return;
-  const int64_t u = i / Bp;
-  const int c = static_cast<int>(i - u * Bp);
-  if (c >= B) {
-    S[i] = 0.f;
-    base[i] = 0.f;
-    C[i] = 0.f;
-    return;
+__global__ void __launch_bounds__(kCopyThreads)
+    batch_init_kernel(int32_t n, int B, int lq, int K, int c0, const int32_t *__restrict__ perm,
+                      const int32_t *__restrict__ rowoff, const int32_t *__restrict__ odeg,
+                      const float *__restrict__ rsum, const float *__restrict__ tele_old,
+                      float uniform, float one_minus_d, float *__restrict__ S,
+                      float *__restrict__ C, float *__restrict__ base, uint8_t *__restrict__ tflag) {
+  const int64_t total = static_cast<int64_t>(n) << lq;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  const int w = 1 << lq;
+  const unsigned grp_mask = (w >= 32 ? 0xffffffffu : ((1u << w) - 1u)) << (lane & ~(w - 1));
+  for (int64_t wb = static_cast<int64_t>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31);
+       wb < total; wb += stride) {
+    const int64_t i = wb + lane;
+    const int64_t u = i >> lq;
+    const bool live = i < total;
+    const int q = static_cast<int>(i & (w - 1));
+    float t[4] = {0.f, 0.f, 0.f, 0.f};
+    bool nz = false;
+    float denom = 1.f;
+    if (live) {
+      const int64_t row = tele_old ? static_cast<int64_t>(perm[u]) * K + c0 : 0;
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const int col = 4 * q + c;
+        if (col < B) t[c] = tele_old ? tele_old[row + col] : uniform;
+        nz |= t[c] != 0.f;
+      }
+      if (W) denom = rsum[u];
+      else if (DIR) denom = __int2float_rn(odeg[u]);
+      else denom = __int2float_rn(rowoff[u + 1] - rowoff[u]);
+    }
+    // any nonzero teleport entry in the row: OR over the row's w lanes
+    const bool row_nz = (__ballot_sync(0xffffffffu, nz) & grp_mask) != 0u;
+    if (live) {
+      const int64_t o = 4 * i;  // = u * Bp + 4 * q
+      *reinterpret_cast<float4 *>(S + o) = make_float4(t[0], t[1], t[2], t[3]);
+      *reinterpret_cast<float4 *>(C + o) =
+          make_float4(__fdiv_rn(t[0], denom), __fdiv_rn(t[1], denom), __fdiv_rn(t[2], denom),
+                      __fdiv_rn(t[3], denom));
+      if (row_nz)
+        *reinterpret_cast<float4 *>(base + o) =
+            make_float4(__fmul_rn(one_minus_d, t[0]), __fmul_rn(one_minus_d, t[1]),
+                        __fmul_rn(one_minus_d, t[2]), __fmul_rn(one_minus_d, t[3]));
+      if (q == 0) tflag[u] = row_nz ? 1 : 0;
+    }
   }
-  const float t = tele_old ? tele_old[static_cast<int64_t>(perm[u]) * K + c0 + c] : uniform;
-  float denom;
-  if (W) denom = rsum[u];
-  else if (DIR) denom = __int2float_rn(odeg[u]);
-  else denom = __int2float_rn(rowoff[u + 1] - rowoff[u]);
-  S[i] = t;
-  base[i] = __fmul_rn(one_minus_d, t);
-  C[i] = __fdiv_rn(t, denom);
 }
 
-// Writes tile columns src.c[j] (j < B) to caller columns dst.c[j], in
-// original vertex ids.
-__global__ void batch_out_kernel(int32_t n, int B, int Bp, int K, ColMap src, ColMap dst,
-                                 const int32_t *__restrict__ inv, const float *__restrict__ S,
-                                 float *out_old) {
-  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= static_cast<int64_t>(n) * B) return;
-  const int64_t v = i / B;
-  const int j = static_cast<int>(i - v * B);
-  out_old[v * K + dst.c[j]] = S[static_cast<int64_t>(inv[v]) * Bp + src.c[j]];
+// Where each tile column's final scores are: block `phase[c]` of the score
+// arena (width W[phase]), column j[c].
+struct OutSrc {
+  const float *S[4];
+  int32_t W[4];
+  int32_t j[kMaxTile];
+  int8_t phase[kMaxTile];
+};
+
+// The tile's write-back: caller column c0 + c of original vertex perm[u]
+// takes tile column c of renumbered row u.  Rows are read in order and every
+// output row is written as one contiguous run of B floats.
+__global__ void __launch_bounds__(kCopyThreads)
+    batch_out_kernel(int32_t n, int B, int lb, int K, int c0, const int32_t *__restrict__ perm,
+                     OutSrc src, float *__restrict__ out_old) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int c = static_cast<int>(t & ((1 << lb) - 1));
+  if (c >= B) return;  // whole-thread exit: no collective below
+  const int64_t ustride = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> lb;
+  const int p = src.phase[c];
+  const float *__restrict__ Sp = src.S[p];
+  const int64_t Wp = src.W[p];
+  const int jc = src.j[c];
+  for (int64_t u0 = t >> lb; u0 < n; u0 += 4 * ustride) {
+    float x[4];
+    int64_t o[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int64_t u = u0 + r * ustride;
+      o[r] = -1;
+      if (u < n) {
+        x[r] = Sp[u * Wp + jc];
+        o[r] = static_cast<int64_t>(perm[u]) * K + c0 + c;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+      if (o[r] >= 0) out_old[o[r]] = x[r];
+  }
+}
+
+// Resets the control block, tickets, sweep counts and trace of a phase.
+__global__ void batch_phase_begin_kernel(BatchCtl *ctl, unsigned long long active, int loops,
+                                         int done, unsigned *tick1, int ngroups, int32_t *sweeps,
+                                         double *trace, int64_t trace_len) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  if (t == 0) {
+    ctl->loop.done = done;
+    ctl->loop.loops = loops;
+    ctl->loop.halted = done;
+    ctl->tick2 = 0;
+    ctl->compact = 0;
+    ctl->active = active;
+  }
+  for (int64_t k = t; k <= ngroups; k += stride) tick1[k] = 0;
+  for (int64_t k = t; k < kMaxTile; k += stride) sweeps[k] = 0;
+  for (int64_t k = t; k < trace_len; k += stride) trace[k] = 0.0;
+}
+
+// Blocks for a copy kernel over `cells` cells: the persistent grid, or fewer
+// when the copy is small.
+unsigned CopyGrid(int64_t cells) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t need = (cells + kCopyThreads - 1) / kCopyThreads;
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(need, sms * kCopyBlocksPerSM)));
+}
+
+int Log2(int x) {
+  int l = 0;
+  while ((1 << l) < x) l++;
+  return l;
 }
 
 template <typename T>
@@ -449,6 +697,14 @@ int GridFor(const void *fn) {
     }                                                                  \
   } while (0)
 
+// Pinned read-back area: control block, per-column sweeps, trace.
+constexpr int64_t kHostSweepsOff = 64;
+constexpr int64_t kHostTraceOff = kHostSweepsOff + sizeof(int32_t) * kMaxTile;
+static_assert(sizeof(BatchCtl) <= kHostSweepsOff, "control block fits its slot");
+int64_t HostBytes(int iters) {
+  return kHostTraceOff + sizeof(double) * static_cast<int64_t>(std::max(iters, 1)) * kMaxTile;
+}
+
 // Buffers for tiles up to kMaxTile columns and a grid of up to nblocks.
 cudaError_t EnsureBatchBuffers(const DeviceGraph &g, BatchScratch &bs, int nblocks, int iters,
                                std::string *err) {
@@ -456,12 +712,12 @@ cudaError_t EnsureBatchBuffers(const DeviceGraph &g, BatchScratch &bs, int nbloc
   const int64_t cells = n * kMaxTile;
   if (!bs.S || bs.cap_cells < cells) {
     int64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
-    for (float **p : {&bs.S, &bs.C[0], &bs.C[1], &bs.base}) {
+    for (float **p : {&bs.S, &bs.C[0], &bs.C[1], &bs.base, &bs.base2}) {
       if (*p) cudaFree(*p);
       *p = nullptr;
     }
-    bs.cap_cells = 0;
-    PB_TRY(GrowB(&bs.S, &c0, cells));
+    bs.cap_cells = bs.cap_cells2 = 0;
+    PB_TRY(GrowB(&bs.S, &c0, 2 * cells));
     PB_TRY(GrowB(&bs.C[0], &c1, cells));
     PB_TRY(GrowB(&bs.C[1], &c2, cells));
     PB_TRY(GrowB(&bs.base, &c3, cells));
@@ -481,7 +737,18 @@ cudaError_t EnsureBatchBuffers(const DeviceGraph &g, BatchScratch &bs, int nbloc
   PB_TRY(GrowB(&bs.trace, &bs.cap_trace, static_cast<int64_t>(std::max(iters, 1)) * kMaxTile));
   if (!bs.sweeps) PB_TRY(cudaMalloc(&bs.sweeps, sizeof(int32_t) * kMaxTile));
   PB_TRY(GrowB(&bs.seg_partial, &bs.cap_seg, std::max<int64_t>(g.num_segments, 1) * kMaxTile));
+  PB_TRY(GrowB(&bs.tflag, &bs.cap_flag, n));
   if (!bs.ctl) PB_TRY(cudaMalloc(&bs.ctl, sizeof(BatchCtl)));
+  const int64_t host_need = HostBytes(iters);
+  if (!bs.host || bs.cap_host < host_need) {
+    if (bs.host) cudaFreeHost(bs.host);
+    bs.host = nullptr;
+    bs.cap_host = 0;
+    PB_TRY(cudaMallocHost(reinterpret_cast<void **>(&bs.host), host_need));
+    bs.cap_host = host_need;
+  }
+  for (cudaEvent_t &e : bs.ev)
+    if (!e) PB_TRY(cudaEventCreate(&e));
   return cudaSuccess;
 }
 
@@ -497,19 +764,19 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
                       const float *tele_old, float *out_old, int32_t *sweeps_tile,
                       double *trace_tile, float *sweep_ms, int64_t *launches, std::string *err) {
   const int64_t n = g.n;
-  const int T = 256;
   const void *fn0 = BatchSweepKernel(g, Bp);
   const int nblocks0 = GridFor(fn0);
   PB_TRY(EnsureBatchBuffers(g, bs, nblocks0, max_iters, err));
-  const unsigned ib = static_cast<unsigned>((n * Bp + T - 1) / T);
+  const int lq = Log2(Bp / 4);
+  const unsigned ib = CopyGrid(n << lq);
   const float uniform = 1.0f / static_cast<float>(n);
   const float omd = 1.0f - damping;
   if (g.weighted)
-    batch_init_kernel<true, false><<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, Bp, K, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base);
+    batch_init_kernel<true, false><<<ib, kCopyThreads, 0, s>>>(static_cast<int32_t>(n), B, lq, K, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base, bs.tflag);
   else if (g.directed)
-    batch_init_kernel<false, true><<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, Bp, K, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base);
+    batch_init_kernel<false, true><<<ib, kCopyThreads, 0, s>>>(static_cast<int32_t>(n), B, lq, K, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base, bs.tflag);
   else
-    batch_init_kernel<false, false><<<ib, T, 0, s>>>(static_cast<int32_t>(n), B, Bp, K, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base);
+    batch_init_kernel<false, false><<<ib, kCopyThreads, 0, s>>>(static_cast<int32_t>(n), B, lq, K, c0, g.perm, g.rowoff, g.odeg, g.rsum, tele_old, uniform, omd, bs.S, bs.C[0], bs.base, bs.tflag);
   PB_TRY(cudaGetLastError());
   *launches += 1;
 
@@ -518,31 +785,30 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
   for (int j = 0; j < kMaxTile; j++) map.c[j] = j < B ? c0 + j : 0;
   int nact = B;                 // columns of the current tile (all iterate at phase start)
   float *S = bs.S, *base = bs.base;
+  int64_t s_off = 0;            // this phase's score block within the arena
+  OutSrc osrc;
+  std::memset(&osrc, 0, sizeof(osrc));
+  int phase = 0;
   float *Cpair[2] = {bs.C[0], bs.C[1]};  // Cpair[k & 1] is gathered by sweep k
   int loops = 0;
   for (int j = 0; j < B; j++) sweeps_tile[j] = 0;
-  std::vector<int32_t> sw(kMaxTile);
-  std::vector<double> tr(static_cast<size_t>(std::max(max_iters, 1)) * kMaxTile);
+  BatchCtl ctl;
+  const int32_t *sw = reinterpret_cast<const int32_t *>(bs.host + kHostSweepsOff);
+  const double *tr = reinterpret_cast<const double *>(bs.host + kHostTraceOff);
   *sweep_ms = 0;
-  cudaEvent_t e0, e1;
-  PB_TRY(cudaEventCreate(&e0));
-  PB_TRY(cudaEventCreate(&e1));
+  cudaEvent_t e0 = bs.ev[0], e1 = bs.ev[1];
   int tile_bp = Bp;
   while (true) {
     const void *fn = BatchSweepKernel(g, tile_bp);
     const int nblocks = GridFor(fn);
     PB_TRY(EnsureBatchBuffers(g, bs, nblocks, max_iters, err));
     const int ngroups = (nblocks + kReduceGroup - 1) / kReduceGroup;
-    BatchCtl ctl0;
-    std::memset(&ctl0, 0, sizeof(ctl0));
-    ctl0.active = (nact == 64) ? ~0ull : ((1ull << nact) - 1ull);
-    ctl0.loop.done = (loops >= max_iters) ? 1 : 0;
-    ctl0.loop.loops = loops;
-    PB_TRY(cudaMemcpyAsync(bs.ctl, &ctl0, sizeof(ctl0), cudaMemcpyHostToDevice, s));
-    PB_TRY(cudaMemsetAsync(bs.tick1, 0, sizeof(unsigned) * (ngroups + 1), s));
-    PB_TRY(cudaMemsetAsync(bs.sweeps, 0, sizeof(int32_t) * kMaxTile, s));
-    if (max_iters)
-      PB_TRY(cudaMemsetAsync(bs.trace, 0, sizeof(double) * static_cast<int64_t>(max_iters) * kMaxTile, s));
+    const unsigned long long active0 = (nact == 64) ? ~0ull : ((1ull << nact) - 1ull);
+    batch_phase_begin_kernel<<<8, 256, 0, s>>>(bs.ctl, active0, loops, loops >= max_iters ? 1 : 0,
+                                               bs.tick1, ngroups, bs.sweeps, bs.trace,
+                                               static_cast<int64_t>(max_iters) * kMaxTile);
+    PB_TRY(cudaGetLastError());
+    *launches += 1;
     BatchArgs a;
     std::memset(&a, 0, sizeof(a));
     a.n = static_cast<int32_t>(n);
@@ -553,6 +819,7 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
     a.odeg = g.odeg;
     a.rsum = g.rsum;
     a.base = base;
+    a.tflag = bs.tflag;
     a.damping = damping;
     a.S = S;
     a.C0 = Cpair[0];
@@ -578,38 +845,36 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
     // gather them (no in-neighbour means no out-neighbour).
     a.zero_final_sweep = g.directed ? loops + 2 : 1;
     a.l1_rows = static_cast<int32_t>(std::min<int64_t>(n, kL1GatherBytes / (4 * tile_bp)));
+    a.hot_rows = static_cast<int32_t>(std::min<int64_t>(n, kL2HotBytes / (4 * tile_bp)));
+    // rows shorter than two rounds of a warp's gathers (2 * kUnroll * 32/L
+    // entries) go one per lane group: bin 1 + log2(L) starts at that length
+    {
+      const int L = tile_bp / 4;
+      int b = 1;
+      for (int l = L; l > 1; l >>= 1) b++;
+      a.short_start = static_cast<int32_t>(g.bin_row_start[b]);
+    }
     a.epsilon = epsilon;
     PB_TRY(cudaEventRecord(e0, s));
     PB_TRY(bs.loop[WidthIndex(tile_bp)].Launch(fn, dim3(nblocks), dim3(kBT), &a, sizeof(a),
                                                &bs.ctl->loop, max_iters, s));
     PB_TRY(cudaEventRecord(e1, s));
-    BatchCtl ctl;
-    PB_TRY(cudaMemcpyAsync(&ctl, bs.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, s));
-    PB_TRY(cudaMemcpyAsync(sw.data(), bs.sweeps, sizeof(int32_t) * nact, cudaMemcpyDeviceToHost, s));
+    PB_TRY(cudaMemcpyAsync(bs.host, bs.ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+    PB_TRY(cudaMemcpyAsync(bs.host + kHostSweepsOff, bs.sweeps, sizeof(int32_t) * nact,
+                           cudaMemcpyDeviceToHost, s));
     if (max_iters && trace_tile)
-      PB_TRY(cudaMemcpyAsync(tr.data(), bs.trace,
+      PB_TRY(cudaMemcpyAsync(bs.host + kHostTraceOff, bs.trace,
                              sizeof(double) * static_cast<int64_t>(max_iters) * tile_bp,
                              cudaMemcpyDeviceToHost, s));
     PB_TRY(cudaStreamSynchronize(s));
-    // write back the columns that are final: those that retired in this
-    // phase, or all of them when the tile is done
-    const bool last_phase = !ctl.compact || ctl.loop.loops >= max_iters;
-    if (out_old) {
-      ColMap fin_src, fin_dst;
-      int nfin = 0;
-      for (int j = 0; j < nact; j++)
-        if (last_phase || !((ctl.active >> j) & 1ull)) {
-          fin_src.c[nfin] = j;
-          fin_dst.c[nfin] = map.c[j];
-          nfin++;
-        }
-      for (int j = nfin; j < kMaxTile; j++) fin_src.c[j] = fin_dst.c[j] = 0;
-      if (nfin) {
-        batch_out_kernel<<<static_cast<unsigned>((n * nfin + T - 1) / T), T, 0, s>>>(
-            static_cast<int32_t>(n), nfin, tile_bp, K, fin_src, fin_dst, g.inv, S, out_old);
-        PB_TRY(cudaGetLastError());
-        *launches += 1;
-      }
+    std::memcpy(&ctl, bs.host, sizeof(ctl));
+    // every column of this phase has its latest scores in this phase's block
+    osrc.S[phase] = S;
+    osrc.W[phase] = tile_bp;
+    for (int j = 0; j < nact; j++) {
+      const int lc = map.c[j] - c0;
+      osrc.phase[lc] = static_cast<int8_t>(phase);
+      osrc.j[lc] = j;
     }
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
@@ -636,21 +901,30 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
       }
     for (int j = m2; j < kMaxTile; j++) src.c[j] = next_map.c[j] = 0;
     const int bn = PadWidth(m2);
-    if (!bs.S2) {
-      int64_t c2a = 0, c2b = 0;
-      PB_TRY(GrowB(&bs.S2, &c2a, n * kMaxTile));
+    if (!bs.base2 || bs.cap_cells2 < n * kMaxTile) {
+      if (bs.base2) cudaFree(bs.base2);
+      bs.base2 = nullptr;
+      int64_t c2b = 0;
       PB_TRY(GrowB(&bs.base2, &c2b, n * kMaxTile));
       bs.cap_cells2 = n * kMaxTile;
     }
-    float *S_new = (S == bs.S) ? bs.S2 : bs.S;
+    const int64_t s_off_new = s_off + n * tile_bp;
+    if (s_off_new + n * bn > 2 * n * kMaxTile || phase + 1 >= 4) {
+      *err = "batched solve: phase blocks exceed the score arena";
+      return cudaErrorInvalidValue;
+    }
+    float *S_new = bs.S + s_off_new;
     float *b_new = (base == bs.base) ? bs.base2 : bs.base;
     float *C_cur = Cpair[loops & 1];
     float *C_new = Cpair[(loops + 1) & 1];  // free: holds contribs two sweeps old
-    batch_repack_kernel<<<static_cast<unsigned>((n * bn + T - 1) / T), T, 0, s>>>(
-        static_cast<int32_t>(n), tile_bp, bn, m2, src, S, base, C_cur, S_new, b_new, C_new);
+    batch_repack_kernel<<<CopyGrid(n * bn), kCopyThreads, 0, s>>>(
+        static_cast<int32_t>(n), tile_bp, Log2(bn), m2, src, bs.tflag, S, base, C_cur, S_new,
+        b_new, C_new);
     PB_TRY(cudaGetLastError());
     *launches += 1;
     S = S_new;
+    s_off = s_off_new;
+    phase++;
     base = b_new;
     Cpair[loops & 1] = C_new;
     Cpair[(loops + 1) & 1] = C_cur;
@@ -658,8 +932,14 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
     nact = m2;
     tile_bp = bn;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  // one write-back of all B columns, each from the block it finished in
+  if (out_old) {
+    const int lb = Log2(B);
+    batch_out_kernel<<<CopyGrid(n << lb), kCopyThreads, 0, s>>>(static_cast<int32_t>(n), B, lb, K,
+                                                                  c0, g.perm, osrc, out_old);
+    PB_TRY(cudaGetLastError());
+    *launches += 1;
+  }
   return cudaSuccess;
 }
 
@@ -698,7 +978,7 @@ cudaError_t TuneTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, flo
 
 void FreeBatchScratch(BatchScratch *b) {
   for (auto &l : b->loop) l.Reset();
-  float **fp[] = {&b->S, &b->C[0], &b->C[1], &b->base, &b->S2, &b->base2, &b->seg_partial};
+  float **fp[] = {&b->S, &b->C[0], &b->C[1], &b->base, &b->base2, &b->seg_partial};
   for (float **p : fp) {
     if (*p) cudaFree(*p);
     *p = nullptr;
@@ -711,9 +991,18 @@ void FreeBatchScratch(BatchScratch *b) {
   if (b->tick1) cudaFree(b->tick1);
   if (b->sweeps) cudaFree(b->sweeps);
   if (b->ctl) cudaFree(b->ctl);
+  if (b->tflag) cudaFree(b->tflag);
+  if (b->host) cudaFreeHost(b->host);
+  for (cudaEvent_t &e : b->ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
   b->tick1 = nullptr;
   b->sweeps = nullptr;
   b->ctl = nullptr;
+  b->tflag = nullptr;
+  b->host = nullptr;
+  b->cap_flag = b->cap_host = 0;
   b->cap_cells = b->cap_cells2 = b->cap_part = b->cap_groups = b->cap_trace = b->cap_seg = 0;
   b->tuned_tile = b->tuned_ncols = 0;
   b->tuned_graph = nullptr;

@@ -24,10 +24,23 @@ struct BatchCtl {
 };
 
 struct BatchScratch {
-  // Two score/base sets: a repack copies the surviving columns of one set
-  // into the other.  The two contrib buffers are shared by both sets.
+  // S is an arena of N x 2*kMaxTile floats: every phase of a tile gets its
+  // own N x width score block in it (widths at least halve from phase to
+  // phase, so they fit), and a column that retires keeps its final scores
+  // in the block of the phase it retired in until the tile's one write-back.
+  // base alternates between two blocks: a repack copies the surviving
+  // columns of one into the other.  The two contrib buffers serve every
+  // phase.  base rows are written and read only where tflag[u] is set (the
+  // row has a nonzero teleport entry in the tile); elsewhere base is zero by
+  // definition.
   float *S = nullptr, *C[2] = {nullptr, nullptr}, *base = nullptr;
-  float *S2 = nullptr, *base2 = nullptr;
+  float *base2 = nullptr;
+  uint8_t *tflag = nullptr;
+  int64_t cap_flag = 0;
+  // pinned host mirror of the phase results (ctl, sweeps, trace)
+  unsigned char *host = nullptr;
+  int64_t cap_host = 0;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
   double *part1 = nullptr, *part2 = nullptr, *trace = nullptr;
   unsigned *tick1 = nullptr;
   int32_t *sweeps = nullptr;

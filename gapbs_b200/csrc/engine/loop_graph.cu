@@ -11,8 +11,11 @@ namespace {
 // Profilers that replay kernels one by one cannot replay kernel nodes inside
 // a graph with conditional nodes.  GAPBS_PR_PLAIN_LAUNCH=1 makes Launch issue
 // the same kernels as ordinary launches instead: max_iters sweep launches
-// (those after convergence return at once) each followed by a one-thread
-// kernel that advances the sweep index.  Results are identical.
+// (those after the loop stopped return at once) each followed by a
+// one-thread kernel that advances the sweep index like the decide kernel:
+// it counts every sweep that ran, including the one that set `done`, none
+// after it, and stops the loop once the sweep index reaches max_iters.
+// Results and sweep counts are identical.
 bool PlainLaunchMode() {
   static const bool plain = [] {
     const char *v = std::getenv("GAPBS_PR_PLAIN_LAUNCH");
@@ -21,8 +24,15 @@ bool PlainLaunchMode() {
   return plain;
 }
 
-__global__ void loop_advance_kernel(LoopCtl *ctl) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) ctl->loops = ctl->loops + 1;
+__global__ void loop_advance_kernel(LoopCtl *ctl, int max_iters) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || ctl->halted) return;
+  const int loops = ctl->loops + 1;
+  ctl->loops = loops;
+  if (ctl->done || loops >= max_iters) {
+    // the decide kernel's stop rule; later sweep launches see done and return
+    ctl->halted = 1;
+    ctl->done = 1;
+  }
 }
 
 __global__ void loop_decide_kernel(LoopCtl *ctl, int max_iters,
@@ -115,7 +125,7 @@ cudaError_t LoopGraph::Launch(const void *fn, dim3 grid, dim3 block, const void 
     for (int i = 0; i < max_iters; i++) {
       cudaError_t e = cudaLaunchKernel(fn, grid, block, params, 0, s);
       if (e != cudaSuccess) return e;
-      loop_advance_kernel<<<1, 32, 0, s>>>(ctl);
+      loop_advance_kernel<<<1, 32, 0, s>>>(ctl, max_iters);
     }
     return cudaGetLastError();
   }

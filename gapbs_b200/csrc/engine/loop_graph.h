@@ -20,8 +20,9 @@ namespace prgpu {
 
 // Shared prefix of every solve's device control block.
 struct LoopCtl {
-  int done;   // set by the sweep kernel when the solve converged
-  int loops;  // sweeps issued so far; owned by the decide kernel
+  int done;    // set by the sweep kernel when the solve converged
+  int loops;   // sweeps issued so far; owned by the decide kernel
+  int halted;  // plain-launch mode: the sweep that set `done` has been counted
 };
 
 class LoopGraph {
