@@ -24,10 +24,16 @@
 // per warp at once, so the per-row work (offsets, old score, update, stores)
 // of the many short rows runs in parallel instead of one row at a time.
 //
-// L2 policy: the first hot_rows rows of the block (the highest in-degree
-// vertices, gathered most often) are written and gathered evict-last; the
-// other rows evict-first, so the streams of cold rows do not push the hub
-// rows out of L2.  The first l1_rows rows are also gathered through L1.
+// Cache policy: contrib rows are written and gathered evict-last in L2 (the
+// index and score streams are evict-first); the first l1_rows rows (the
+// highest in-degree vertices, gathered most often) are gathered through L1,
+// all others bypass it so they cannot evict the hubs.
+//
+// Occupancy: the sweep is bound by the latency of its gathers, not by L2 or
+// HBM bandwidth (a 64-column sweep moves ~7 TB/s from L2, a fifth of what the
+// L2-to-SM path carries), so the kernel is compiled for 8 resident blocks per
+// SM (6 for weighted graphs) even though that spills a few registers to L1:
+// more warps in flight beat the spill traffic.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,11 +51,6 @@ constexpr int kBT = 256;       // threads per block
 constexpr int kBW = kBT / 32;  // warps per block
 constexpr int kUnroll = 4;     // gather instructions in flight per lane
 constexpr int64_t kL1GatherBytes = 96 * 1024;  // L1 budget for hub rows per SM
-#ifndef GAPBS_BATCH_L2_HOT_MB
-#define GAPBS_BATCH_L2_HOT_MB 80
-#endif
-// L2 budget for the evict-last hub rows of the contrib block.
-constexpr int64_t kL2HotBytes = static_cast<int64_t>(GAPBS_BATCH_L2_HOT_MB) << 20;
 
 struct BatchArgs {
   int32_t n;
@@ -83,7 +84,6 @@ struct BatchArgs {
   int32_t zero_final_sweep;  // first sweep that may skip rows without in-neighbours
   int32_t l1_rows;  // rows [0, l1_rows) (the hubs) are gathered through L1; the
                     // rest bypass it so they cannot evict the hubs
-  int32_t hot_rows;     // rows [0, hot_rows) are kept in L2 (evict-last)
   int32_t short_start;  // rows [short_start, n) go one row per lane group
   double epsilon;
 };
@@ -104,14 +104,13 @@ __device__ __forceinline__ float4 f4add(float4 a, float4 b) {
   return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
 }
 
-// Loads columns 4*gl .. 4*gl+3 of contrib row v with the row's cache policy.
+// Loads columns 4*gl .. 4*gl+3 of contrib row v (through L1 for hub rows).
 __device__ __forceinline__ float4 gather_row4(const BatchArgs &a, const float *Cin, int v, int gl,
-                                              uint64_t ps, uint64_t pg) {
+                                              uint64_t pg) {
   // element offset < 2^32 (n * 64 fits while n < 2^26)
   const float4 *src = reinterpret_cast<const float4 *>(
       Cin + (static_cast<uint32_t>(v) * static_cast<uint32_t>(a.Bp) + 4u * gl));
-  const uint64_t pol = v < a.hot_rows ? pg : ps;
-  return v < a.l1_rows ? ld_gather_v4(src, pol) : ld_gather_v4_cold(src, pol);
+  return v < a.l1_rows ? ld_gather_v4(src, pg) : ld_gather_v4_cold(src, pg);
 }
 
 // Sum over entries [s, e) of w_e * Cin[v_e, 4*gl .. 4*gl+3], where lane group
@@ -145,7 +144,7 @@ __device__ __forceinline__ float4 row_accumulate(const BatchArgs &a, const float
         const int v = __shfl_sync(0xffffffffu, idx, kk & 31);
         wk[q] = W ? __shfl_sync(0xffffffffu, w, kk & 31) : 1.f;
         x[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (gather && kk < cnt) x[q] = gather_row4(a, Cin, v, gl, ps, pg);
+        if (gather && kk < cnt) x[q] = gather_row4(a, Cin, v, gl, pg);
       }
 #pragma unroll
       for (int q = 0; q < kUnroll; q++) {
@@ -212,7 +211,7 @@ __device__ __forceinline__ float4 group_accumulate(const BatchArgs &a, const flo
           const int v = __shfl_sync(0xffffffffu, idx[kk / L], srcl);
           wk[q] = W ? __shfl_sync(0xffffffffu, w[kk / L], srcl) : 1.f;
           x[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (gather && j0 + kk < len) x[q] = gather_row4(a, Cin, v, gl, ps, pg);
+          if (gather && j0 + kk < len) x[q] = gather_row4(a, Cin, v, gl, pg);
         }
 #pragma unroll
         for (int q = 0; q < kUnroll; q++) {
@@ -258,7 +257,7 @@ __device__ __forceinline__ void finish4(const BatchArgs &a, float *Cout, int u, 
 }
 
 template <int L, bool W, bool DIR>
-__global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
+__global__ void __launch_bounds__(kBT, W ? 6 : 8) batch_sweep_kernel(const BatchArgs a) {
   if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
   const int it = *reinterpret_cast<volatile const int *>(&a.ctl->loop.loops);
   const float *Cin = (it & 1) ? a.C1 : a.C0;
@@ -353,7 +352,7 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
     if (lane < L && gather) {
       if (fl) bs = ld_stream_v4f(reinterpret_cast<const float4 *>(a.base + i), ps);
       finish4<W, DIR>(a, Cout, u, gl, active4, acc, old, bs, bdenom<W, DIR>(a, u), err, ps,
-                      u < a.hot_rows ? pg : ps);
+                      pg);
     }
   }
   {
@@ -379,7 +378,7 @@ __global__ void __launch_bounds__(kBT) batch_sweep_kernel(const BatchArgs a) {
       if (valid && gather) {
         if (fl) bs = ld_stream_v4f(reinterpret_cast<const float4 *>(a.base + i), ps);
         finish4<W, DIR>(a, Cout, u, gl, active4, acc, old, bs, bdenom<W, DIR>(a, u), err, ps,
-                        u < a.hot_rows ? pg : ps);
+                        pg);
       }
     }
   }
@@ -845,7 +844,6 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
     // gather them (no in-neighbour means no out-neighbour).
     a.zero_final_sweep = g.directed ? loops + 2 : 1;
     a.l1_rows = static_cast<int32_t>(std::min<int64_t>(n, kL1GatherBytes / (4 * tile_bp)));
-    a.hot_rows = static_cast<int32_t>(std::min<int64_t>(n, kL2HotBytes / (4 * tile_bp)));
     // rows shorter than two rounds of a warp's gathers (2 * kUnroll * 32/L
     // entries) go one per lane group: bin 1 + log2(L) starts at that length
     {
