@@ -45,6 +45,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_pr_verify_f32.restype = c_double
         L.oracle_pr_residual_f64.argtypes = [c_int64, P, P, P, c_float, P]
         L.oracle_pr_residual_f64.restype = c_double
+        L.oracle_ppr_residual_f64.argtypes = [c_int64, P, P, P, c_float, P, P]
+        L.oracle_ppr_residual_f64.restype = c_double
         L.oracle_ppr_f64.argtypes = [c_int64, P, P, P, P, P, c_double, P, c_int, c_double, P, P]
         L.oracle_ppr_f64.restype = c_int
         L.oracle_ppr_f64_from.argtypes = [c_int64, P, P, P, P, P, c_double, P, P, c_int, c_double, P, P]
@@ -95,6 +97,15 @@ def pr_residual_f64(g, scores, damping=0.85) -> float:
     n, io, inb, oo, _ = _csr(g)
     s = np.ascontiguousarray(scores, np.float32)
     return float(lib().oracle_pr_residual_f64(n, _ptr(io), _ptr(inb), _ptr(oo), damping, _ptr(s)))
+
+
+def ppr_residual_f64(g, t, s, damping=0.85) -> float:
+    """L1 residual of one PPR score column (unit weights); see pr_oracle.h."""
+    n, io, inb, oo, _ = _csr(g)
+    t = np.ascontiguousarray(t, np.float32)
+    s = np.ascontiguousarray(s, np.float32)
+    return float(lib().oracle_ppr_residual_f64(n, _ptr(io), _ptr(inb), _ptr(oo), damping,
+                                               _ptr(t), _ptr(s)))
 
 
 def ppr_f64(n, in_off, in_nbr, out_off, t, in_w=None, rowsum=None, damping=0.85,

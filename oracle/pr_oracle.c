@@ -114,6 +114,23 @@ double oracle_pr_residual_f64(int64_t n, const int64_t *in_off,
   return error;
 }
 
+double oracle_ppr_residual_f64(int64_t n, const int64_t *in_off,
+                               const int32_t *in_nbr, const int64_t *out_off,
+                               float damping, const float *t, const float *s) {
+  const double d = (double)damping;
+  double error = 0;
+  #pragma omp parallel for reduction(+ : error) schedule(dynamic, 4096)
+  for (int64_t u = 0; u < n; u++) {
+    double acc = 0;
+    for (int64_t e = in_off[u]; e < in_off[u + 1]; e++) {
+      int32_t v = in_nbr[e];
+      acc += (double)s[v] / (double)deg_of(out_off, v);
+    }
+    error += fabs((1.0 - d) * (double)t[u] + d * acc - (double)s[u]);
+  }
+  return error;
+}
+
 /* Row sums S_v: explicit or out-degree. */
 static inline double rowsum_of(const double *rowsum, const int64_t *out_off,
                                int64_t v) {

@@ -56,6 +56,14 @@ double oracle_pr_residual_f64(int64_t n, const int64_t *in_off,
                               const int32_t *in_nbr, const int64_t *out_off,
                               float damping, const float *scores);
 
+/* Double-precision personalized-PageRank residual
+ *   sum_u |(1-d) t[u] + d * sum_{v in in(u)} s[v]/outdeg(v) - s[u]|
+ * of one FP32 score column s for teleport column t (unit weights).  After a
+ * Jacobi sweep whose L1 change was c, the residual is at most d * c. */
+double oracle_ppr_residual_f64(int64_t n, const int64_t *in_off,
+                               const int32_t *in_nbr, const int64_t *out_off,
+                               float damping, const float *t, const float *s);
+
 /* Personalized PageRank, one column, FP64.
  *   s = (1-d) t + d P^T s,  P[v,u] = w(v->u) / S_v,  S_v = sum_u w(v->u)
  * in_w (nullable => unit weights) holds w(v->u) aligned with in_nbr (the

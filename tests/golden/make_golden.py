@@ -15,8 +15,20 @@ from its own sources by oracle/Makefile) exist.  Writes:
   adversarial.npz                    small hand-made edge lists (isolated
                                      vertices, star hub, chain, directed sinks)
                                      with the reference's scores on each
+  pr_fullsize.json                   (--fullsize) the benchmark-size graphs
+                                     (-u 24 -k 16, -g 25 -k 16, and the graphs
+                                     of the PPR and adjoint workloads): graph
+                                     identity, the reference's sweep count and
+                                     -l lines, top-5, PRVerifier line, and its
+                                     float32 scores at 4096 fixed sample
+                                     vertices
 
-Usage:  python tests/golden/make_golden.py
+  cli_golden.json                    (--cli) the reference pr_spmv's exit code
+                                     and stdout for -h and for rejected
+                                     invocations (missing file, unknown
+                                     suffix, missing or unknown option)
+
+Usage:  python tests/golden/make_golden.py [--fullsize | --cli]
 """
 from __future__ import annotations
 
@@ -169,5 +181,91 @@ def main():
         json.dump(out, fh, indent=1)
 
 
+# (case name, pr_spmv arguments, run PageRankPull)
+FULLSIZE_CASES = [
+    ("u24", "-u 24 -k 16", True),
+    ("g25", "-g 25 -k 16", True),
+    ("g22", "-g 22", True),
+    ("g20", "-g 20", False),
+]
+SAMPLE_SEED = 27491095 + 2
+SAMPLE_COUNT = 4096
+
+
+def sample_vertices(n: int) -> np.ndarray:
+    """Fixed sample: the 64 lowest ids, then uniform ids, sorted, unique."""
+    rng = np.random.default_rng(SAMPLE_SEED)
+    ids = np.concatenate([np.arange(min(64, n)), rng.integers(0, n, SAMPLE_COUNT)])
+    return np.unique(ids)[:SAMPLE_COUNT]
+
+
+def main_fullsize():
+    if not oracle.ref_available():
+        sys.exit("needs oracle/_ref (make -C oracle where the reference tree exists)")
+    out = {"generator": "tests/golden/make_golden.py --fullsize", "sample_seed": SAMPLE_SEED,
+           "cases": {}}
+    for name, args, run in FULLSIZE_CASES:
+        g, _ = capture_stdout(oracle.RefGraph.build, args)
+        oo, onb, io, inb = g.csr()
+        entry = {
+            "args": args,
+            "num_nodes": g.num_nodes,
+            "num_edges": g.num_edges,
+            "num_edges_directed": g.num_edges_directed,
+            "directed": g.directed,
+            "csr_sha256": sha(oo, onb, io, inb),
+        }
+        del oo, onb, io, inb
+        if run:
+            scores, log = capture_stdout(g.pagerank_pull, 20, 1e-4, True)
+            step_lines = [ln for ln in log.splitlines() if ln.strip()]
+            ok, vlog = capture_stdout(g.verify, scores, 1e-4)
+            order = np.lexsort((np.arange(scores.size), -scores.astype(np.float64)))[:5]
+            ids = sample_vertices(g.num_nodes)
+            entry.update({
+                "sweeps": len(step_lines),
+                "log_lines": step_lines,
+                "scores_sum": float(scores.astype(np.float64).sum()),
+                "top5": [[int(i), float(scores[i])] for i in order],
+                "verify_pass": ok,
+                "verify_line": vlog.strip(),
+                "sample_ids": [int(i) for i in ids],
+                "sample_scores": [float(scores[i]) for i in ids],
+            })
+        out["cases"][name] = entry
+        print(name, g.num_nodes, g.num_edges_directed, entry.get("sweeps"), flush=True)
+        del g
+    with open(os.path.join(HERE, "pr_fullsize.json"), "w") as fh:
+        json.dump(out, fh, indent=1)
+
+
+# pr_spmv invocations that end before any kernel runs; {tmp} is a scratch
+# directory holding an empty file x.foo
+CLI_CASES = ["-h", "-f {tmp}/missing.el", "-f {tmp}/x.foo", "-g", "-z", "-n"]
+
+
+def main_cli():
+    import subprocess
+    exe = os.path.join(ROOT, "oracle", "_ref", "pr_spmv")
+    if not os.path.exists(exe):
+        sys.exit("needs oracle/_ref/pr_spmv (make -C oracle where the reference tree exists)")
+    out = {"generator": "tests/golden/make_golden.py --cli", "cases": []}
+    with tempfile.TemporaryDirectory() as tmp:
+        open(os.path.join(tmp, "x.foo"), "w").close()
+        for args in CLI_CASES:
+            p = subprocess.run([exe] + args.format(tmp=tmp).split(), capture_output=True, text=True)
+            out["cases"].append({"args": args, "returncode": p.returncode,
+                                 "stdout": p.stdout.replace(tmp, "{tmp}")})
+            print(args, p.returncode)
+    with open(os.path.join(HERE, "cli_golden.json"), "w") as fh:
+        json.dump(out, fh, indent=1)
+
+
 if __name__ == "__main__":
-    main()
+    if "--fullsize" in sys.argv[1:]:
+        main_fullsize()
+    elif "--cli" in sys.argv[1:]:
+        main_cli()
+    else:
+        main()
+        main_cli()

@@ -1,0 +1,54 @@
+"""pr_gpu end to end on the GPU, the way the reference's test/test.mk runs
+pr_spmv: the verification line, the -l step lines and the -a top scores.
+"""
+import json
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import GOLDEN, ROOT, gpu_available
+
+pytestmark = pytest.mark.gpu
+EXE = os.path.join(ROOT, "gapbs_b200", "bin", "pr_gpu")
+with open(os.path.join(GOLDEN, "pr_golden.json")) as fh:
+    GOLD = json.load(fh)["cases"]
+STEP = re.compile(r"^ {4}\d+ +\d+\.\d{5}$")
+TOP = re.compile(r"^(\d+):(\S+)$")
+
+
+@pytest.fixture(scope="module")
+def exe():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    if not os.path.exists(EXE):
+        subprocess.run(["make", "-C", ROOT, "cli"], check=True)
+    return EXE
+
+
+def run(exe, args):
+    p = subprocess.run([exe] + args, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    return p.stdout
+
+
+@pytest.mark.parametrize("args,trials", [("-g 10 -n 1 -v", 1), ("-u 10 -n 2 -v", 2),
+                                          ("-g 12 -n 1 -v -i 30 -t 1e-6", 1)])
+def test_verification_passes(exe, args, trials):
+    out = run(exe, args.split())
+    assert out.count("Verification:           PASS") == trials
+    assert "FAIL" not in out
+    assert "Upload Time:" in out and "Average Time:" in out
+
+
+def test_log_lines_and_top_scores(exe):
+    e = GOLD["el4"]
+    out = run(exe, ["-f", os.path.join(GOLDEN, "graphs", "4.el"), "-n", "1", "-v", "-a", "-l"])
+    lines = out.splitlines()
+    assert [ln for ln in lines if STEP.match(ln)] == e["log_lines"]
+    assert "Verification:           PASS" in out
+    top = [TOP.match(ln) for ln in lines if TOP.match(ln)]
+    assert [int(t.group(1)) for t in top] == [v for v, _ in e["top5"]]
+    for t, (_, sc) in zip(top, e["top5"]):
+        assert abs(float(t.group(2)) - sc) <= 1e-5 * sc
