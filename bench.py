@@ -373,8 +373,8 @@ def run_ours(a, dist: Dist):
                 "peak": round(gather_peak / 1e9, 2),
                 "unit": "G gathers/s",
                 "frac": round(gather_achieved / gather_peak, 4),
-                "peak_source": "measured in this run: random 4-byte loads bypassing L1 "
-                               "from a 64 MB (L2-resident) array",
+                "peak_source": "measured in this run: random 4-byte loads (ld.global.nc) "
+                               "from a 64 MB L2-resident array",
             },
         },
         "clocks": clk,
