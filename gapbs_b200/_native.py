@@ -41,6 +41,12 @@ def graph_lib() -> ctypes.CDLL:
         lib.gapbs_graph_build.restype = c_int
         lib.gapbs_graph_from_edges.argtypes = [POINTER(P), P, P, c_int64, c_int]
         lib.gapbs_graph_from_edges.restype = c_int
+        lib.gapbs_graph_new_undirected.argtypes = [POINTER(P), c_int64, c_int64,
+                                                   POINTER(POINTER(c_int64)),
+                                                   POINTER(POINTER(c_int32))]
+        lib.gapbs_graph_new_undirected.restype = c_int
+        lib.gapbs_rmat_permutation.argtypes = [c_int, P]
+        lib.gapbs_rmat_permutation.restype = c_int
         lib.gapbs_graph_write_sg.argtypes = [P, c_char_p]
         lib.gapbs_graph_write_sg.restype = c_int
         lib.gapbs_graph_free.argtypes = [P]

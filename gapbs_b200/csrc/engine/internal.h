@@ -158,6 +158,14 @@ cudaError_t BuildDeviceGraph(DeviceGraph *g, int64_t n, int64_t m,
                              cudaStream_t s, std::string *err);
 void FreeDeviceGraph(DeviceGraph *g);
 
+// The reference's -g / -u graph built on the device (generate.cu): CSR of
+// the symmetrised, squished graph in original ids, int32 offsets (n+1) and
+// neighbours (m), owned by the caller.  perm_host: the R-MAT relabelling.
+cudaError_t GenerateGraph(bool uniform, int scale, int degree, const int32_t *perm_host,
+                          cudaStream_t s, int64_t *n_out, int64_t *m_out, int32_t **off_out,
+                          int32_t **nbr_out, std::string *err);
+void WidenOffsets(int64_t n1, const int32_t *off32, int64_t *off64, cudaStream_t s);
+
 // Warp tasks per bin (fills task_start, returns the total) and the
 // persistent grid size of a sweep kernel (SMs x resident blocks per SM).
 int PullTasks(const DeviceGraph &g, int32_t task_start[kNumBins + 1]);

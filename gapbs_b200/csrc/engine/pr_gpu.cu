@@ -36,6 +36,9 @@ struct pr_gpu {
   static constexpr size_t kChunk = 32u << 20;
   void *pinned[2] = {nullptr, nullptr};
   cudaEvent_t pin_ev[2] = {};
+  // CSR of the last pr_gpu_generate (original ids), kept for download
+  int32_t *gen_off = nullptr, *gen_nbr = nullptr;
+  int64_t gen_n = 0, gen_m = 0;
 };
 
 namespace {
@@ -74,6 +77,13 @@ void HostCopy(void *dst, const void *src, size_t bytes) {
     });
   }
   for (auto &x : th) x.join();
+}
+
+void FreeGenerated(pr_gpu_t *h) {
+  if (h->gen_off) cudaFree(h->gen_off);
+  if (h->gen_nbr) cudaFree(h->gen_nbr);
+  h->gen_off = h->gen_nbr = nullptr;
+  h->gen_n = h->gen_m = 0;
 }
 
 int EnsurePinned(pr_gpu_t *h) {
@@ -405,6 +415,7 @@ void pr_gpu_destroy(pr_gpu_t *h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  FreeGenerated(h);
   h->loop_single.Reset();
   h->loop_adjoint.Reset();
   prgpu::FreeDeviceGraph(&h->g);
@@ -424,6 +435,57 @@ const char *pr_gpu_last_error(const pr_gpu_t *h) {
   return h ? h->err.c_str() : "invalid handle";
 }
 
+int pr_gpu_generate(pr_gpu_t *h, int uniform, int scale, int degree, const int32_t *perm,
+                    int64_t *n_out, int64_t *m_out) {
+  if (!h) return PR_GPU_EINVAL;
+  if (scale < 1 || scale > 30 || degree < 0)
+    return SetErr(h, PR_GPU_EINVAL, "need 1 <= scale <= 30 and degree >= 0");
+  if ((int64_t(2) * degree) << scale > 0x7fffffffLL - 8)
+    return SetErr(h, PR_GPU_ERANGE, "graph exceeds int32 offsets");
+  if (!uniform && !perm) return SetErr(h, PR_GPU_EINVAL, "R-MAT needs the vertex permutation");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  h->has_graph = false;
+  prgpu::FreeDeviceGraph(&h->g);
+  FreeGenerated(h);
+  std::string msg;
+  int64_t n = 0, m = 0;
+  int32_t *off = nullptr, *nbr = nullptr;
+  cudaError_t e = prgpu::GenerateGraph(uniform != 0, scale, degree, perm, h->stream, &n, &m, &off,
+                                       &nbr, &msg);
+  if (e != cudaSuccess)
+    return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
+  h->gen_off = off;
+  h->gen_nbr = nbr;
+  h->gen_n = n;
+  h->gen_m = m;
+  e = prgpu::BuildDeviceGraph(&h->g, n, m, off, nbr, off, nbr, nullptr, false, h->stream, &msg);
+  if (e != cudaSuccess) {
+    FreeGenerated(h);
+    return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
+  }
+  h->has_graph = true;
+  if (n_out) *n_out = n;
+  if (m_out) *m_out = m;
+  return PR_GPU_OK;
+}
+
+int pr_gpu_download_csr(pr_gpu_t *h, int64_t *out_off, int32_t *out_nbr) {
+  if (!h) return PR_GPU_EINVAL;
+  if (!h->gen_off) return SetErr(h, PR_GPU_ENOGRAPH, "no generated graph to download");
+  if (!out_off || (h->gen_m > 0 && !out_nbr)) return SetErr(h, PR_GPU_EINVAL, "null CSR array");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  int64_t *off64 = nullptr;
+  PR_CHECK(h, cudaMalloc(&off64, sizeof(int64_t) * (h->gen_n + 1)));
+  prgpu::WidenOffsets(h->gen_n + 1, h->gen_off, off64, h->stream);
+  cudaError_t e = cudaGetLastError();
+  int rc = e == cudaSuccess ? PR_GPU_OK : CudaErr(h, e, "widen offsets");
+  if (!rc) rc = CopyToHost(h, out_off, off64, sizeof(int64_t) * (h->gen_n + 1));
+  if (!rc) rc = CopyToHost(h, out_nbr, h->gen_nbr, sizeof(int32_t) * h->gen_m);
+  cudaFree(off64);
+  if (!rc) FreeGenerated(h);
+  return rc;
+}
+
 int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m, const int32_t *out_off,
                   const int32_t *out_nbr, const int32_t *in_off, const int32_t *in_nbr,
                   const float *edge_w) {
@@ -437,6 +499,7 @@ int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m, const int32_t *out_off,
   PR_CHECK(h, cudaSetDevice(h->device));
   h->has_graph = false;
   prgpu::FreeDeviceGraph(&h->g);
+  FreeGenerated(h);
   int32_t *d_oo = nullptr, *d_on = nullptr, *d_io = nullptr, *d_in = nullptr;
   float *d_w = nullptr;
   auto release = [&]() {

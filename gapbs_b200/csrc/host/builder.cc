@@ -240,10 +240,7 @@ EdgeList GenerateRMat(int scale, int degree) {
   }
   // Relabel through a seeded random permutation (src/generator.h:93-103).
   Buffer<NodeID> perm(n);
-  #pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < n; i++) perm[i] = static_cast<NodeID>(i);
-  std::mt19937 prng(static_cast<uint32_t>(kRandSeed));
-  std::shuffle(perm.data(), perm.data() + n, prng);
+  RMatPermutation(scale, perm.data());
   #pragma omp parallel for schedule(static)
   for (int64_t e = 0; e < m; e++) {
     el.u[e] = perm[el.u[e]];
@@ -391,6 +388,14 @@ void ParseMTX(std::istream &in, EdgeVec *ev) {
 }
 
 }  // namespace
+
+void RMatPermutation(int scale, NodeID *perm) {
+  const int64_t n = int64_t(1) << scale;
+  #pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; i++) perm[i] = static_cast<NodeID>(i);
+  std::mt19937 prng(static_cast<uint32_t>(kRandSeed));
+  std::shuffle(perm, perm + n, prng);
+}
 
 // ---- serialized graphs (.sg) ---------------------------------------------
 

@@ -52,6 +52,10 @@ HostGraph MakeGraph(const GraphSource &src, bool verbose);
 HostGraph MakeGraphFromEdges(const NodeID *u, const NodeID *v, int64_t m,
                              bool symmetrize);
 
+// The seeded vertex permutation R-MAT graphs are relabelled through
+// (src/generator.h:93-103): perm[i] for i < 2^scale.
+void RMatPermutation(int scale, NodeID *perm);
+
 // Writes / reads the .sg layout of src/writer.h:39-69.
 void WriteSerialized(const HostGraph &g, const std::string &path);
 HostGraph ReadSerialized(const std::string &path);

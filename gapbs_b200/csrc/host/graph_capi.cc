@@ -70,6 +70,30 @@ int gapbs_graph_from_edges(gapbs_graph_t **out, const int32_t *u,
   }
 }
 
+int gapbs_graph_new_undirected(gapbs_graph_t **out, int64_t n, int64_t m, int64_t **off,
+                               int32_t **nbr) {
+  if (!out || !off || !nbr || n < 1 || m < 0) return Fail(-1, "invalid argument");
+  *out = nullptr;
+  try {
+    gapbs_b200::Buffer<gapbs_b200::Offset> o(static_cast<size_t>(n + 1));
+    gapbs_b200::Buffer<gapbs_b200::NodeID> b(static_cast<size_t>(m > 0 ? m : 1));
+    *off = o.data();
+    *nbr = b.data();
+    gapbs_graph *h = new gapbs_graph();
+    h->g = gapbs_b200::HostGraph::Undirected(n, std::move(o), std::move(b));
+    *out = h;
+    return 0;
+  } catch (const std::bad_alloc &) {
+    return Fail(-12, "out of host memory for the graph");
+  }
+}
+
+int gapbs_rmat_permutation(int scale, int32_t *perm) {
+  if (!perm || scale < 0 || scale > 30) return Fail(-1, "invalid argument");
+  gapbs_b200::RMatPermutation(scale, perm);
+  return 0;
+}
+
 int gapbs_graph_write_sg(const gapbs_graph_t *g, const char *path) {
   if (!g || !path) return Fail(-1, "null argument");
   try {

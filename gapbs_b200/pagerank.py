@@ -21,7 +21,7 @@ from typing import Optional
 import numpy as np
 
 from . import _pr_abi
-from ._native import pr_lib
+from ._native import graph_lib, pr_lib
 from .graph import Graph
 
 K_DAMP = np.float32(0.85)   # kDamp, src/pr_spmv.cc:33
@@ -108,6 +108,54 @@ class PageRankEngine:
                             g.in_neighbors, edge_w)
         else:
             self.upload_csr(g.num_nodes, g.out_offsets, g.out_neighbors, None, None, edge_w)
+
+    def generate(self, args: str):
+        """Builds pr_spmv's synthetic graph ("-g SCALE [-k DEGREE]" or
+        "-u SCALE [-k DEGREE]") on the device, identical to the reference's,
+        and uploads it.  Returns (num_nodes, CSR entries)."""
+        toks = args.split()
+        kind = scale = None
+        degree = 16
+        i = 0
+        while i < len(toks):
+            if toks[i] in ("-g", "-u") and i + 1 < len(toks):
+                kind, scale = toks[i], int(toks[i + 1])
+                i += 2
+            elif toks[i] == "-k" and i + 1 < len(toks):
+                degree = int(toks[i + 1])
+                i += 2
+            else:
+                raise ValueError(f"generate takes -g/-u SCALE [-k DEGREE], got {args!r}")
+        if kind is None:
+            raise ValueError("generate needs -g SCALE or -u SCALE")
+        perm = None
+        if kind == "-g":
+            perm = np.empty(1 << scale, np.int32)
+            if graph_lib().gapbs_rmat_permutation(scale, _ptr(perm)) != 0:
+                raise ValueError(f"invalid scale {scale}")
+        n, m = ctypes.c_int64(), ctypes.c_int64()
+        rc = self._lib.pr_gpu_generate(self._h, int(kind == "-u"), scale, degree, _ptr(perm),
+                                       byref(n), byref(m))
+        self._check(rc, "pr_gpu_generate")
+        self.n, self.m = int(n.value), int(m.value)
+        self.directed = False
+        self.weighted = False
+        return self.n, self.m
+
+    def download_graph(self) -> Graph:
+        """The last generated graph as a host Graph (frees its device copy)."""
+        lib = graph_lib()
+        h = ctypes.c_void_p()
+        off = ctypes.POINTER(ctypes.c_int64)()
+        nbr = ctypes.POINTER(ctypes.c_int32)()
+        if lib.gapbs_graph_new_undirected(byref(h), self.n, self.m, byref(off), byref(nbr)) != 0:
+            raise MemoryError("host graph allocation failed")
+        rc = self._lib.pr_gpu_download_csr(self._h, ctypes.cast(off, ctypes.c_void_p),
+                                           ctypes.cast(nbr, ctypes.c_void_p))
+        if rc != 0:
+            lib.gapbs_graph_free(h)
+            self._check(rc, "pr_gpu_download_csr")
+        return Graph(h)
 
     # -- solves ---------------------------------------------------------------
     def run(self, max_iters: int = 20, epsilon: float = 1e-4, damping: float = float(K_DAMP),

@@ -37,6 +37,17 @@ int gapbs_graph_build(gapbs_graph_t **out, const char *args, int verbose);
 int gapbs_graph_from_edges(gapbs_graph_t **out, const int32_t *u,
                            const int32_t *v, int64_t m, int symmetrize);
 
+/* An undirected graph of n vertices and m CSR entries whose arrays the
+ * caller fills (for example from pr_gpu_download_csr): *off receives the
+ * n + 1 offsets, *nbr the m neighbours, both owned by the graph. */
+int gapbs_graph_new_undirected(gapbs_graph_t **out, int64_t n, int64_t m,
+                               int64_t **off, int32_t **nbr);
+
+/* The seeded permutation the reference relabels R-MAT graphs through
+ * (src/generator.h:93-103): perm[i] for i < 2^scale (input of
+ * pr_gpu_generate). */
+int gapbs_rmat_permutation(int scale, int32_t *perm);
+
 /* Writes the .sg serialized layout (src/writer.h:39-69). */
 int gapbs_graph_write_sg(const gapbs_graph_t *g, const char *path);
 

@@ -70,6 +70,26 @@ int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m,
                   const int32_t *in_off, const int32_t *in_nbr,
                   const float *edge_w);
 
+/* Builds the reference's synthetic graph on the device and uploads it as
+ * pr_gpu_upload would: pr_spmv -g scale -k degree (R-MAT, quadrant
+ * probabilities 0.57/0.19/0.19) or, with uniform != 0, -u scale -k degree;
+ * 2^scale * degree edges from the reference's per-block mt19937 streams
+ * (src/generator.h:105-155), symmetrised and squished as its builder does
+ * (src/builder.h:141-170,300-323).  The CSR is identical to the reference's.
+ * R-MAT ids are relabelled through the reference's seeded permutation, which
+ * the caller computes on the host (gapbs_rmat_permutation in gapbs_graph.h,
+ * 2^scale entries); uniform graphs pass NULL.  Replaces the Generator /
+ * BuilderBase::MakeGraph path of src/builder.h:343-364 for -g / -u.
+ *   n_out  vertices (largest id + 1)    m_out  CSR entries (both directions)
+ * The original-id CSR stays on the device until pr_gpu_download_csr, the
+ * next upload or generate, or pr_gpu_destroy. */
+int pr_gpu_generate(pr_gpu_t *h, int uniform, int scale, int degree,
+                    const int32_t *perm, int64_t *n_out, int64_t *m_out);
+
+/* Copies the CSR of the last pr_gpu_generate to host buffers (n_out + 1
+ * offsets, m_out neighbours), then frees the device copy. */
+int pr_gpu_download_csr(pr_gpu_t *h, int64_t *out_off, int32_t *out_nbr);
+
 /* Runs Jacobi PageRank sweeps until the L1 change of a sweep is < epsilon or
  * max_iters sweeps have run (src/pr_spmv.cc:41-58).
  *

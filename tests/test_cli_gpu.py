@@ -39,7 +39,7 @@ def test_verification_passes(exe, args, trials):
     out = run(exe, args.split())
     assert out.count("Verification:           PASS") == trials
     assert "FAIL" not in out
-    assert "Upload Time:" in out and "Average Time:" in out
+    assert "Generate Time:" in out and "Build Time:" in out and "Average Time:" in out
 
 
 def test_log_lines_and_top_scores(exe):
@@ -48,6 +48,7 @@ def test_log_lines_and_top_scores(exe):
     lines = out.splitlines()
     assert [ln for ln in lines if STEP.match(ln)] == e["log_lines"]
     assert "Verification:           PASS" in out
+    assert "Upload Time:" in out
     top = [TOP.match(ln) for ln in lines if TOP.match(ln)]
     assert [int(t.group(1)) for t in top] == [v for v, _ in e["top5"]]
     for t, (_, sc) in zip(top, e["top5"]):

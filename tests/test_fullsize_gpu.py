@@ -85,6 +85,17 @@ def test_pagerankpull_fullsize(engine, case):
     assert oracle.pr_verify_f32(g, s) < 1e-4
 
 
+@pytest.mark.parametrize("case", ["u24", "g25"])
+def test_device_generated_fullsize_graph(engine, case):
+    e = FULL[case]
+    n, m = engine.generate(e["args"])
+    assert (n, m) == (e["num_nodes"], e["num_edges_directed"])
+    res = engine.run(20, 1e-4, 0.85)
+    assert int(res.sweeps[0]) == e["sweeps"]
+    g = engine.download_graph()
+    assert csr_sha(g) == e["csr_sha256"]
+
+
 def test_batched_ppr_fullsize(engine):
     g, _ = load("g22")
     engine.upload(g)
