@@ -205,6 +205,13 @@ def sweep_bytes(n: int, m: int, directed: bool) -> int:
     return b
 
 
+def synthetic(args_str: str) -> bool:
+    """-g / -u graphs are generated on the GPU (pr_gpu_generate)."""
+    toks = args_str.split()
+    return bool(toks) and toks[0] in ("-g", "-u") and all(t in ("-g", "-u", "-k") or t.isdigit()
+                                                          for t in toks)
+
+
 def shm_graph_path(args_str: str) -> str:
     h = hashlib.sha1(args_str.encode()).hexdigest()[:12]
     base = "/dev/shm" if os.path.isdir("/dev/shm") else tempfile.gettempdir()
@@ -253,15 +260,23 @@ def run_ours(a, dist: Dist):
     from gapbs_b200 import PageRankEngine
     dev = dist.local_rank
     torch.cuda.set_device(dev)
-    t0 = time.perf_counter()
-    g = load_graph(a.graph, dist)
-    build_s = time.perf_counter() - t0
-    n, m = g.num_nodes, g.num_edges_directed
     eng = PageRankEngine(dev)
-    t0 = time.perf_counter()
-    eng.upload(g)
-    upload_s = time.perf_counter() - t0
-    upload_bytes = 4 * (n + 1) + 4 * m
+    g = None
+    if synthetic(a.graph):
+        # the reference's -g / -u graph, built on this GPU (identical CSR)
+        t0 = time.perf_counter()
+        n, m = eng.generate(a.graph)
+        build_s = time.perf_counter() - t0
+        upload_s, upload_bytes, directed = 0.0, 0, False
+    else:
+        t0 = time.perf_counter()
+        g = load_graph(a.graph, dist)
+        build_s = time.perf_counter() - t0
+        n, m, directed = g.num_nodes, g.num_edges_directed, g.directed
+        t0 = time.perf_counter()
+        eng.upload(g)
+        upload_s = time.perf_counter() - t0
+        upload_bytes = 4 * (n + 1) + 4 * m
     stream = torch.cuda.current_stream(dev)
     eng.set_stream(stream.cuda_stream)
     out = torch.empty(n, dtype=torch.float32, device=f"cuda:{dev}")
@@ -318,7 +333,7 @@ def run_ours(a, dist: Dist):
 
     # ---- roofline of the fused sweep kernel
     peak, peak_src = measured_peak()
-    bps = sweep_bytes(n, m, g.directed)
+    bps = sweep_bytes(n, m, directed)
     avg_sweep_ms = sweep_ms_total / max(sweeps_total, 1)
     achieved = bps / (avg_sweep_ms / 1e3) / 1e9
     traffic = profiled_traffic(a.graph)
@@ -349,12 +364,15 @@ def run_ours(a, dist: Dist):
             "l2": "256 MB buffer written between steps; graph 4M+4N bytes >> 126 MB L2",
             "parallelism": f"replicas{dist.world}" if dist.world > 1 else "single GPU",
             "graph_build_s": round(build_s, 2),
+            "graph_built_on": "gpu (pr_gpu_generate)" if g is None else "host",
         },
         "e2e": {
             "value": round(e2e_value, 3), "unit": "GTEPS",
             "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4 * n,
             "path": "pr_gpu_run (C ABI, host scores buffer, pinned)",
             "upload_once_s": round(upload_s, 3), "upload_once_bytes": upload_bytes,
+            "graph_note": ("generated on the device once before timing"
+                           if g is None else "uploaded once before timing"),
             "ms_per_step": round(e2e_s * 1e3 / a.steps, 4),
         },
         "roofline": {
@@ -388,6 +406,8 @@ def run_ours(a, dist: Dist):
 
     # ---- CPU baseline on this host (rank 0 at N=1 only)
     if not a.no_cpu_baseline and dist.rank == 0 and dist.world == 1:
+        if g is None:
+            g = eng.download_graph()  # the generated graph, for the reference on the host
         result["cpu_baseline"] = cpu_baseline(g, a, sweeps_per_step)
     eng.close()
     return result
@@ -397,11 +417,15 @@ def run_ppr(a, dev):
     import torch
     from gapbs_b200 import PageRankEngine
     from gapbs_b200.graph import make_graph
-    g = make_graph(a.ppr_graph)
+    eng = PageRankEngine(dev)
+    if synthetic(a.ppr_graph):
+        eng.generate(a.ppr_graph)
+        g = eng.download_graph()  # host copy for the seed sets
+    else:
+        g = make_graph(a.ppr_graph)
+        eng.upload(g)
     n, m = g.num_nodes, g.num_edges_directed
     T, sizes = ppr_teleports(g, a.ppr_cols, seed=27491095 + 1)
-    eng = PageRankEngine(dev)
-    eng.upload(g)
     stream = torch.cuda.current_stream(dev)
     eng.set_stream(stream.cuda_stream)
     Td = torch.from_numpy(T).to(f"cuda:{dev}")
