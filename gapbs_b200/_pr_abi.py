@@ -15,7 +15,7 @@ PR_GPU_ERANGE = -6
 
 # Every symbol include/pr_gpu.h declares.
 SYMBOLS = (
-    "pr_gpu_create", "pr_gpu_upload", "pr_gpu_generate", "pr_gpu_download_csr",
+    "pr_gpu_create", "pr_gpu_upload", "pr_gpu_upload_sg", "pr_gpu_generate", "pr_gpu_download_csr",
     "pr_gpu_run", "pr_gpu_run_device",
     "pr_gpu_adjoint", "pr_gpu_adjoint_device", "pr_gpu_set_stream",
     "pr_gpu_set_batch_tile", "pr_gpu_get_batch_tile", "pr_gpu_last_timing",
@@ -28,6 +28,8 @@ def declare(lib):
     lib.pr_gpu_create.restype = c_int
     lib.pr_gpu_upload.argtypes = [P, c_int64, c_int64, P, P, P, P, P]
     lib.pr_gpu_upload.restype = c_int
+    lib.pr_gpu_upload_sg.argtypes = [P, c_char_p]
+    lib.pr_gpu_upload_sg.restype = c_int
     lib.pr_gpu_generate.argtypes = [P, c_int, c_int, c_int, P, POINTER(c_int64), POINTER(c_int64)]
     lib.pr_gpu_generate.restype = c_int
     lib.pr_gpu_download_csr.argtypes = [P, P, P]

@@ -346,6 +346,27 @@ void WidenOffsets(int64_t n1, const int32_t *off32, int64_t *off64, cudaStream_t
   widen_offsets_kernel<<<GridFor(n1), 256, 0, s>>>(n1, off32, off64);
 }
 
+namespace {
+__global__ void narrow_offsets_kernel(int64_t count, const int64_t *__restrict__ wide,
+                                      int32_t *__restrict__ narrow, int *bad) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+       i += stride) {
+    const int64_t v = wide[i];
+    if (v < 0 || v > 0x7fffffffLL) {
+      *bad = 1;
+      narrow[i] = 0;
+    } else {
+      narrow[i] = static_cast<int32_t>(v);
+    }
+  }
+}
+}  // namespace
+
+void NarrowOffsets(int64_t count, const int64_t *wide, int32_t *narrow, int *bad, cudaStream_t s) {
+  narrow_offsets_kernel<<<GridFor(count), 256, 0, s>>>(count, wide, narrow, bad);
+}
+
 #undef GEN_TRY
 
 }  // namespace prgpu

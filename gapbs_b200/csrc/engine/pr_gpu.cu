@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
@@ -96,10 +97,28 @@ int EnsurePinned(pr_gpu_t *h) {
   return PR_GPU_OK;
 }
 
-// Host -> device through two pinned chunks (host copy of chunk k+1 overlaps
-// the DMA of chunk k).
+// True when [p, p + bytes) starts and ends in page-locked host memory
+// (cudaMallocHost, cudaHostRegister, torch pin_memory): such buffers are
+// copied by DMA directly, without the staging chunks.
+bool PageLocked(const void *p, size_t bytes) {
+  cudaPointerAttributes a0, a1;
+  if (cudaPointerGetAttributes(&a0, p) != cudaSuccess ||
+      cudaPointerGetAttributes(&a1, static_cast<const char *>(p) + bytes - 1) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a0.type == cudaMemoryTypeHost && a1.type == cudaMemoryTypeHost;
+}
+
+// Host -> device: page-locked sources by one DMA; others through two pinned
+// chunks (host copy of chunk k+1 overlaps the DMA of chunk k).
 int CopyToDevice(pr_gpu_t *h, void *dst, const void *src, size_t bytes) {
   if (bytes == 0) return PR_GPU_OK;
+  if (PageLocked(src, bytes)) {
+    PR_CHECK(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream));
+    PR_CHECK(h, cudaStreamSynchronize(h->stream));
+    return PR_GPU_OK;
+  }
   int rc = EnsurePinned(h);
   if (rc) return rc;
   size_t off = 0;
@@ -118,9 +137,15 @@ int CopyToDevice(pr_gpu_t *h, void *dst, const void *src, size_t bytes) {
   return PR_GPU_OK;
 }
 
-// Device -> host through the pinned chunks.
+// Device -> host: page-locked destinations by one DMA; others through the
+// pinned chunks.
 int CopyToHost(pr_gpu_t *h, void *dst, const void *src, size_t bytes) {
   if (bytes == 0) return PR_GPU_OK;
+  if (PageLocked(dst, bytes)) {
+    PR_CHECK(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+    PR_CHECK(h, cudaStreamSynchronize(h->stream));
+    return PR_GPU_OK;
+  }
   int rc = EnsurePinned(h);
   if (rc) return rc;
   size_t off = 0, pend_off = 0, pend_len = 0;
@@ -484,6 +509,120 @@ int pr_gpu_download_csr(pr_gpu_t *h, int64_t *out_off, int32_t *out_nbr) {
   cudaFree(off64);
   if (!rc) FreeGenerated(h);
   return rc;
+}
+
+// Streams count elements of `elem` bytes from f to dst on the device through
+// the two pinned chunks (the read of chunk k+1 overlaps the DMA of chunk k).
+// narrow != nullptr: the elements are int64 offsets, DMA'd to `wide` (one
+// chunk of device staging) and narrowed into narrow[] on the device, with
+// *bad set for values outside [0, 2^31).
+static int StreamFileToDevice(pr_gpu_t *h, FILE *f, int64_t count, size_t elem, void *dst,
+                       int64_t *wide, int32_t *narrow, int *bad, const char *what) {
+  int rc = EnsurePinned(h);
+  if (rc) return rc;
+  const size_t chunk = pr_gpu::kChunk / elem;
+  int64_t done = 0;
+  int k = 0;
+  while (done < count) {
+    const size_t len = static_cast<size_t>(std::min<int64_t>(chunk, count - done));
+    PR_CHECK(h, cudaEventSynchronize(h->pin_ev[k]));
+    if (std::fread(h->pinned[k], elem, len, f) != len)
+      return SetErr(h, PR_GPU_EGRAPH, std::string("truncated serialized graph (") + what + ")");
+    if (narrow) {
+      // one device staging chunk: wait for the previous narrowing to finish
+      PR_CHECK(h, cudaStreamSynchronize(h->stream));
+      PR_CHECK(h, cudaMemcpyAsync(wide, h->pinned[k], len * elem, cudaMemcpyHostToDevice,
+                                  h->stream));
+      prgpu::NarrowOffsets(static_cast<int64_t>(len), wide, narrow + done, bad, h->stream);
+      PR_CHECK(h, cudaGetLastError());
+    } else {
+      PR_CHECK(h, cudaMemcpyAsync(static_cast<char *>(dst) + done * elem, h->pinned[k], len * elem,
+                                  cudaMemcpyHostToDevice, h->stream));
+    }
+    PR_CHECK(h, cudaEventRecord(h->pin_ev[k], h->stream));
+    done += static_cast<int64_t>(len);
+    k ^= 1;
+  }
+  return PR_GPU_OK;
+}
+
+int pr_gpu_upload_sg(pr_gpu_t *h, const char *path) {
+  if (!h || !path) return PR_GPU_EINVAL;
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return SetErr(h, PR_GPU_EINVAL, std::string("couldn't open file ") + path);
+  unsigned char directed_byte = 0;
+  int64_t entries = 0, n = 0;
+  const bool header = std::fread(&directed_byte, 1, 1, f) == 1 &&
+                      std::fread(&entries, sizeof(int64_t), 1, f) == 1 &&
+                      std::fread(&n, sizeof(int64_t), 1, f) == 1;
+  if (!header || n < 1 || entries < 0) {
+    std::fclose(f);
+    return SetErr(h, PR_GPU_EGRAPH, std::string("corrupt serialized graph ") + path);
+  }
+  if (n > 0x7fffffffLL - 1 || entries > 0x7fffffffLL - 8) {
+    std::fclose(f);
+    return SetErr(h, PR_GPU_ERANGE, "graph exceeds int32 ids / offsets");
+  }
+  const bool directed = directed_byte != 0;
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) {
+    std::fclose(f);
+    return CudaErr(h, e, "cudaSetDevice");
+  }
+  h->has_graph = false;
+  prgpu::FreeDeviceGraph(&h->g);
+  FreeGenerated(h);
+  int32_t *d_oo = nullptr, *d_on = nullptr, *d_io = nullptr, *d_in = nullptr;
+  int64_t *wide = nullptr;
+  int *bad = nullptr;
+  auto release = [&]() {
+    cudaStreamSynchronize(h->stream);  // no copy into these buffers is in flight
+    for (void *p : {static_cast<void *>(d_oo), static_cast<void *>(d_on),
+                    static_cast<void *>(d_io), static_cast<void *>(d_in),
+                    static_cast<void *>(wide), static_cast<void *>(bad)})
+      if (p) cudaFree(p);
+    std::fclose(f);
+  };
+  e = cudaMalloc(&d_oo, sizeof(int32_t) * (n + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&d_on, sizeof(int32_t) * std::max<int64_t>(entries, 1));
+  if (e == cudaSuccess && directed) e = cudaMalloc(&d_io, sizeof(int32_t) * (n + 1));
+  if (e == cudaSuccess && directed)
+    e = cudaMalloc(&d_in, sizeof(int32_t) * std::max<int64_t>(entries, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&wide, pr_gpu::kChunk);
+  if (e == cudaSuccess) e = cudaMalloc(&bad, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int), h->stream);
+  if (e != cudaSuccess) {
+    release();
+    return CudaErr(h, e, "device allocation for upload");
+  }
+  int rc = StreamFileToDevice(h, f, n + 1, sizeof(int64_t), nullptr, wide, d_oo, bad, "offsets");
+  if (!rc) rc = StreamFileToDevice(h, f, entries, sizeof(int32_t), d_on, nullptr, nullptr, nullptr,
+                                   "neighbours");
+  if (!rc && directed)
+    rc = StreamFileToDevice(h, f, n + 1, sizeof(int64_t), nullptr, wide, d_io, bad, "offsets");
+  if (!rc && directed)
+    rc = StreamFileToDevice(h, f, entries, sizeof(int32_t), d_in, nullptr, nullptr, nullptr,
+                            "neighbours");
+  int hbad = 0;
+  if (!rc) {
+    e = cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = CudaErr(h, e, "reading the offsets check");
+  }
+  if (!rc && hbad) rc = SetErr(h, PR_GPU_EGRAPH, "invalid CSR: offsets outside int32");
+  if (rc) {
+    release();
+    return rc;
+  }
+  std::string msg;
+  e = prgpu::BuildDeviceGraph(&h->g, n, entries, d_oo, d_on, directed ? d_io : d_oo,
+                              directed ? d_in : d_on, nullptr, directed, h->stream, &msg);
+  release();
+  if (e == cudaErrorInvalidValue && !msg.empty() && msg.rfind("invalid CSR", 0) == 0)
+    return SetErr(h, PR_GPU_EGRAPH, msg);
+  if (e != cudaSuccess) return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
+  h->has_graph = true;
+  return PR_GPU_OK;
 }
 
 int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m, const int32_t *out_off,

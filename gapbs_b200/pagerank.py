@@ -14,6 +14,7 @@ adjoint, timing and graph facts.
 from __future__ import annotations
 
 import ctypes
+import os
 from ctypes import byref, c_double, c_int64
 from dataclasses import dataclass
 from typing import Optional
@@ -108,6 +109,19 @@ class PageRankEngine:
                             g.in_neighbors, edge_w)
         else:
             self.upload_csr(g.num_nodes, g.out_offsets, g.out_neighbors, None, None, edge_w)
+
+    def upload_sg(self, path: str):
+        """Uploads a serialized (.sg) graph file straight to the device (no host
+        CSR); returns (num_nodes, CSR entries)."""
+        rc = self._lib.pr_gpu_upload_sg(self._h, os.fsencode(path))
+        self._check(rc, "pr_gpu_upload_sg")
+        with open(path, "rb") as fh:
+            head = fh.read(17)  # bool directed, int64 entries, int64 n
+        self.directed = head[0] != 0
+        self.m = int.from_bytes(head[1:9], "little", signed=True)
+        self.n = int.from_bytes(head[9:17], "little", signed=True)
+        self.weighted = False
+        return self.n, self.m
 
     def generate(self, args: str):
         """Builds pr_spmv's synthetic graph ("-g SCALE [-k DEGREE]" or

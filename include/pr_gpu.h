@@ -70,6 +70,15 @@ int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m,
                   const int32_t *in_off, const int32_t *in_nbr,
                   const float *edge_w);
 
+/* Uploads a serialized graph file (.sg, the layout of src/writer.h:39-69 that
+ * the reference's reader loads in src/reader.h:254-307) straight from the
+ * file to the device: the file is read in chunks into pinned buffers and
+ * copied by DMA while the next chunk is read; int64 offsets are narrowed to
+ * int32 on the device.  No host copy of the CSR is built.  Same validation
+ * and result as pr_gpu_upload of the same graph; a truncated or corrupt file
+ * returns PR_GPU_EGRAPH. */
+int pr_gpu_upload_sg(pr_gpu_t *h, const char *path);
+
 /* Builds the reference's synthetic graph on the device and uploads it as
  * pr_gpu_upload would: pr_spmv -g scale -k degree (R-MAT, quadrant
  * probabilities 0.57/0.19/0.19) or, with uniform != 0, -u scale -k degree;
