@@ -55,6 +55,8 @@ def parse_args():
     p.add_argument("--ppr-graph", default="-g 22")
     p.add_argument("--ppr-cols", type=int, default=64)
     p.add_argument("--no-ppr", action="store_true")
+    p.add_argument("--adjoint-graph", default="-g 20")
+    p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-trials", type=int, default=2)
     return p.parse_args()
@@ -403,6 +405,8 @@ def run_ours(a, dist: Dist):
     # ---- batched PPR vs sequential single-vector solves (rank 0, N=1 config)
     if not a.no_ppr and dist.rank == 0:
         result["ppr"] = run_ppr(a, dev)
+    if not a.no_adjoint and dist.rank == 0:
+        result["adjoint"] = run_adjoint(a, dev)
 
     # ---- CPU baseline on this host (rank 0 at N=1 only)
     if not a.no_cpu_baseline and dist.rank == 0 and dist.world == 1:
@@ -467,9 +471,24 @@ def run_ppr(a, dev):
         eng.run_device(a.max_iters, a.epsilon, 0.85, 1, cols[c].data_ptr(), out1.data_ptr())
         maxdiff = max(maxdiff, float((out[:, c] - out1).abs().sum()))
     eng.close()
+    # Roofline of the batched solve: every column-sweep gathers 4 bytes per
+    # edge (one float of each neighbour's contrib row, served mostly by L2);
+    # the streams are ids and offsets once per sweep step and old score, new
+    # score and next contrib (12 bytes) per vertex and column-sweep.
+    col_sweeps = float(bsweeps.sum())
+    steps = float(bsweeps.max())
+    gathered = 4.0 * m * col_sweeps
+    streamed = steps * (4.0 * m + 4.0 * (n + 1)) + 12.0 * n * col_sweeps
     return {
         "workload": f"{a.ppr_cols} PPR vectors on {a.ppr_graph.strip()} (N={n}, M={m}), seed sets "
                     f"log-uniform in [1,4096] (sizes min {min(sizes)} max {max(sizes)})",
+        "roofline": {
+            "kernel": "batch_sweep_kernel",
+            "gathered_gbs": round(gathered / (b_ms / 1e3) / 1e9, 1),
+            "streamed_gbs": round(streamed / (b_ms / 1e3) / 1e9, 1),
+            "note": "gathered bytes come mostly from L2 (78 % hit, profiles/"
+                    "batch_sweep_g20_full.md); the sweep is bound by gather latency",
+        },
         "batched_gteps": round(b_gteps, 3),
         "batched_ms": round(b_ms, 3),
         "batched_sweeps_total": int(bsweeps.sum()),
@@ -478,6 +497,56 @@ def run_ppr(a, dev):
         "sequential_sweeps_total": ssweeps,
         "speedup_aggregate_gteps": round(b_gteps / s_gteps, 3),
         "max_l1_batched_vs_single": maxdiff,
+    }
+
+
+def run_adjoint(a, dev):
+    """Reverse-mode solve of L = w . s on a weighted graph: forward PPR, then
+    the adjoint sweeps and the edge-weight gradient pass, timed with CUDA
+    events (host buffers excluded: device-pointer entry points)."""
+    import torch
+    from gapbs_b200 import PageRankEngine
+    eng = PageRankEngine(dev)
+    eng.generate(a.adjoint_graph)
+    g = eng.download_graph()
+    n, m = g.num_nodes, g.num_edges_directed
+    rng = np.random.default_rng(27491095 + 3)
+    ew = rng.uniform(0.5, 1.5, m).astype(np.float32)
+    eng.upload(g, edge_w=ew)
+    stream = torch.cuda.current_stream(dev)
+    eng.set_stream(stream.cuda_stream)
+    t = torch.from_numpy(ppr_teleports(g, 1, seed=27491095 + 3)[0][:, 0].copy()).to(f"cuda:{dev}")
+    s = torch.empty(n, dtype=torch.float32, device=f"cuda:{dev}")
+    w = torch.from_numpy(rng.normal(size=n).astype(np.float32)).to(f"cuda:{dev}")
+    gt = torch.empty(n, dtype=torch.float32, device=f"cuda:{dev}")
+    ge = torch.empty(m, dtype=torch.float32, device=f"cuda:{dev}")
+    fsw = asw = 0
+    for _ in range(max(1, a.warmup)):
+        eng.run_device(100, 1e-7, 0.85, 1, t.data_ptr(), s.data_ptr())
+        eng.adjoint_device(300, 1e-7, 0.85, w.data_ptr(), s.data_ptr(), gt.data_ptr(),
+                           ge.data_ptr())
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    fsw, _ = eng.run_device(100, 1e-7, 0.85, 1, t.data_ptr(), s.data_ptr())
+    e1.record(stream)
+    asw = eng.adjoint_device(300, 1e-7, 0.85, w.data_ptr(), s.data_ptr(), gt.data_ptr(),
+                             ge.data_ptr())
+    e2.record(stream)
+    torch.cuda.synchronize()
+    f_ms, a_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    eng.close()
+    asw = int(asw)
+    # adjoint sweeps read ids, weights and offsets of the out-rows (8M + 4(N+1))
+    # plus 16N of vectors; the gradient pass reads 8M and writes 4M
+    adj_bytes = asw * (8.0 * m + 4.0 * (n + 1) + 16.0 * n) + 12.0 * m
+    return {
+        "workload": f"weighted PPR adjoint on {a.adjoint_graph} (N={n}, M={m}), weights "
+                    f"U[0.5,1.5], loss weights N(0,1), epsilon 1e-7",
+        "forward_sweeps": int(fsw[0]), "forward_ms": round(f_ms, 3),
+        "adjoint_sweeps": asw, "adjoint_ms": round(a_ms, 3),
+        "adjoint_gteps": round(m * asw / (a_ms / 1e3) / 1e9, 2),
+        "adjoint_algorithmic_gbs": round(adj_bytes / (a_ms / 1e3) / 1e9, 1),
     }
 
 
