@@ -239,7 +239,7 @@ __device__ __forceinline__ float comp(const float4 &v, int c) {
 template <bool W, bool DIR>
 __device__ __forceinline__ void finish4(const BatchArgs &a, float *Cout, int u, int gl,
                                         unsigned active4, float4 sum, float4 old, float4 bs,
-                                        float den, double err[4], uint64_t ps, uint64_t pl) {
+                                        float den, double *err, uint64_t ps, uint64_t pl) {
   const int64_t i = static_cast<int64_t>(u) * a.Bp + 4 * gl;
   float nw[4], cv[4];
   // one division per row; contrib = new * (1 / S_v) is within an ulp of new / S_v
@@ -250,7 +250,7 @@ __device__ __forceinline__ void finish4(const BatchArgs &a, float *Cout, int u, 
     const bool act = (active4 >> c) & 1u;
     nw[c] = act ? __fadd_rn(comp(bs, c), __fmul_rn(a.damping, comp(sum, c))) : o;
     cv[c] = __fmul_rn(nw[c], inv);
-    if (act) err[c] += static_cast<double>(fabsf(__fsub_rn(nw[c], o)));
+    if (act) err[c * kBT] += static_cast<double>(fabsf(__fsub_rn(nw[c], o)));
   }
   st_hint_v4(reinterpret_cast<float4 *>(a.S + i), make_float4(nw[0], nw[1], nw[2], nw[3]), ps);
   st_hint_v4(reinterpret_cast<float4 *>(Cout + i), make_float4(cv[0], cv[1], cv[2], cv[3]), pl);
@@ -275,7 +275,12 @@ __global__ void __launch_bounds__(kBT, W ? 6 : 8) batch_sweep_kernel(const Batch
       *reinterpret_cast<volatile const unsigned long long *>(&a.ctl->active);
   const unsigned active4 = static_cast<unsigned>((active >> (4 * gl)) & 0xFull);
   const bool gather = active4 != 0u;
-  double err[4] = {0, 0, 0, 0};
+  // per-thread FP64 error of its four columns, in shared memory (column c of
+  // thread t at s_err[c][t]) to keep registers for gathers in flight
+  __shared__ double s_err[4][kBT];
+  double *err = &s_err[0][threadIdx.x];
+#pragma unroll
+  for (int c = 0; c < 4; c++) err[c * kBT] = 0.0;
   if (threadIdx.x < kMaxTile) scol[threadIdx.x] = 0;
 
   // ---- hub segments, block-cooperative
@@ -341,16 +346,12 @@ __global__ void __launch_bounds__(kBT, W ? 6 : 8) batch_sweep_kernel(const Batch
   for (int u = a.hub_rows + gw; u < warp_end; u += nw) {
     float4 old = make_float4(0.f, 0.f, 0.f, 0.f), bs = old;
     const int64_t i = static_cast<int64_t>(u) * Bp + 4 * gl;
-    int fl = 0;
-    if (lane < L && gather) {  // issued before the gathers, consumed after
-      old = ld_score_v4(reinterpret_cast<const float4 *>(a.S + i), ps);
-      fl = __ldg(a.tflag + u);
-    }
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     if (u < a.zero_start)
       acc = row_accumulate<L, W>(a, Cin, a.rowoff[u], a.rowoff[u + 1], lane, gather, ps, pg);
     if (lane < L && gather) {
-      if (fl) bs = ld_stream_v4f(reinterpret_cast<const float4 *>(a.base + i), ps);
+      old = ld_score_v4(reinterpret_cast<const float4 *>(a.S + i), ps);
+      if (__ldg(a.tflag + u)) bs = ld_stream_v4f(reinterpret_cast<const float4 *>(a.base + i), ps);
       finish4<W, DIR>(a, Cout, u, gl, active4, acc, old, bs, bdenom<W, DIR>(a, u), err, ps,
                       pg);
     }
@@ -369,30 +370,28 @@ __global__ void __launch_bounds__(kBT, W ? 6 : 8) batch_sweep_kernel(const Batch
       }
       float4 old = make_float4(0.f, 0.f, 0.f, 0.f), bs = old;
       const int64_t i = static_cast<int64_t>(u) * Bp + 4 * gl;
-      int fl = 0;
-      if (valid && gather) {
-        old = ld_score_v4(reinterpret_cast<const float4 *>(a.S + i), ps);
-        fl = __ldg(a.tflag + u);
-      }
       const float4 acc = group_accumulate<L, W>(a, Cin, s, len, lane, gather, ps, pg);
       if (valid && gather) {
-        if (fl) bs = ld_stream_v4f(reinterpret_cast<const float4 *>(a.base + i), ps);
+        old = ld_score_v4(reinterpret_cast<const float4 *>(a.S + i), ps);
+        if (__ldg(a.tflag + u)) bs = ld_stream_v4f(reinterpret_cast<const float4 *>(a.base + i), ps);
         finish4<W, DIR>(a, Cout, u, gl, active4, acc, old, bs, bdenom<W, DIR>(a, u), err, ps,
                         pg);
       }
     }
   }
   // lane groups hold partial errors of the same columns: combine them
+  double errc[4];
 #pragma unroll
   for (int c = 0; c < 4; c++) {
+    errc[c] = err[c * kBT];
 #pragma unroll
-    for (int o = L; o < 32; o <<= 1) err[c] += __shfl_xor_sync(0xffffffffu, err[c], o);
+    for (int o = L; o < 32; o <<= 1) errc[c] += __shfl_xor_sync(0xffffffffu, errc[c], o);
   }
 
   // ---- per-column block partial, then two-stage grid reduction per column
   if (lane < L) {
 #pragma unroll
-    for (int c = 0; c < 4; c++) serr[wid][4 * gl + c] = err[c];
+    for (int c = 0; c < 4; c++) serr[wid][4 * gl + c] = errc[c];
   }
   __syncthreads();
   const int b = blockIdx.x;
