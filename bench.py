@@ -57,6 +57,8 @@ def parse_args():
     p.add_argument("--no-ppr", action="store_true")
     p.add_argument("--adjoint-graph", default="-g 20")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--e2e-upload-steps", type=int, default=3,
+                   help="steps of the end-to-end variant that uploads the graph every step")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-trials", type=int, default=2)
     return p.parse_args()
@@ -333,6 +335,32 @@ def run_ours(a, dist: Dist):
     e2e_edges = dist.sum(float(m) * e2e_sweeps)
     e2e_value = e2e_edges / e2e_s / 1e9
 
+    # ---- end to end with the graph uploaded every step (a caller whose graph
+    # changes between solves): pr_gpu_upload of the host CSR + pr_gpu_run
+    e2e_up = None
+    if a.e2e_upload_steps > 0:
+        if g is None:
+            g = eng.download_graph()  # the generated graph, as a host CSR
+        up_s, up_sweeps = 0.0, 0
+        for i in range(a.e2e_upload_steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.upload(g)
+            res = eng.run(a.max_iters, a.epsilon, out=host_out)
+            dt = time.perf_counter() - t0
+            if i > 0:  # the first is a warm-up
+                up_s += dt
+                up_sweeps += int(res.sweeps[0])
+        up_s = dist.max(up_s)
+        e2e_up = {
+            "value": round(dist.sum(float(m) * up_sweeps) / up_s / 1e9, 3), "unit": "GTEPS",
+            "h2d_bytes_per_step": 4 * (n + 1) + 4 * m, "d2h_bytes_per_step": 4 * n,
+            "path": "pr_gpu_upload (host CSR, pageable) + pr_gpu_run every step",
+            "ms_per_step": round(up_s * 1e3 / a.e2e_upload_steps, 3),
+            "steps": a.e2e_upload_steps,
+        }
+        eng.set_stream(stream.cuda_stream)
+
     # ---- roofline of the fused sweep kernel
     peak, peak_src = measured_peak()
     bps = sweep_bytes(n, m, directed)
@@ -400,6 +428,8 @@ def run_ours(a, dist: Dist):
         "clocks": clk,
         "gpu_launches": int(launches),
     }
+    if e2e_up is not None:
+        result["e2e_graph_upload_each_step"] = e2e_up
     del flush
 
     # ---- batched PPR vs sequential single-vector solves (rank 0, N=1 config)

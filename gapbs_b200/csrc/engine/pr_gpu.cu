@@ -68,8 +68,9 @@ void HostCopy(void *dst, const void *src, size_t bytes) {
     std::memcpy(dst, src, bytes);
     return;
   }
-  const int nt = 4;
-  std::thread th[nt];
+  static const int nt = static_cast<int>(
+      std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2)));
+  std::thread th[8];
   const size_t per = (bytes + nt - 1) / nt;
   for (int t = 0; t < nt; t++) {
     const size_t lo = std::min(bytes, per * t), hi = std::min(bytes, per * (t + 1));
@@ -77,7 +78,7 @@ void HostCopy(void *dst, const void *src, size_t bytes) {
       std::memcpy(static_cast<char *>(dst) + lo, static_cast<const char *>(src) + lo, hi - lo);
     });
   }
-  for (auto &x : th) x.join();
+  for (int t = 0; t < nt; t++) th[t].join();
 }
 
 void FreeGenerated(pr_gpu_t *h) {
