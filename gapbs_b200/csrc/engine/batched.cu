@@ -105,11 +105,13 @@ __device__ __forceinline__ float4 f4add(float4 a, float4 b) {
 }
 
 // Loads columns 4*gl .. 4*gl+3 of contrib row v (through L1 for hub rows).
+// The offset is counted in float4 units in 32 bits: the host keeps
+// n * L below 2^32 (MaxTileFor).
+template <int L>
 __device__ __forceinline__ float4 gather_row4(const BatchArgs &a, const float *Cin, int v, int gl,
                                               uint64_t pg) {
-  // element offset < 2^32 (n * 64 fits while n < 2^26)
-  const float4 *src = reinterpret_cast<const float4 *>(
-      Cin + (static_cast<uint32_t>(v) * static_cast<uint32_t>(a.Bp) + 4u * gl));
+  const float4 *src = reinterpret_cast<const float4 *>(Cin) +
+                      (static_cast<uint32_t>(v) * static_cast<uint32_t>(L) + static_cast<uint32_t>(gl));
   return v < a.l1_rows ? ld_gather_v4(src, pg) : ld_gather_v4_cold(src, pg);
 }
 
@@ -144,7 +146,7 @@ __device__ __forceinline__ float4 row_accumulate(const BatchArgs &a, const float
         const int v = __shfl_sync(0xffffffffu, idx, kk & 31);
         wk[q] = W ? __shfl_sync(0xffffffffu, w, kk & 31) : 1.f;
         x[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (gather && kk < cnt) x[q] = gather_row4(a, Cin, v, gl, pg);
+        if (gather && kk < cnt) x[q] = gather_row4<L>(a, Cin, v, gl, pg);
       }
 #pragma unroll
       for (int q = 0; q < kUnroll; q++) {
@@ -211,7 +213,7 @@ __device__ __forceinline__ float4 group_accumulate(const BatchArgs &a, const flo
           const int v = __shfl_sync(0xffffffffu, idx[kk / L], srcl);
           wk[q] = W ? __shfl_sync(0xffffffffu, w[kk / L], srcl) : 1.f;
           x[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (gather && j0 + kk < len) x[q] = gather_row4(a, Cin, v, gl, pg);
+          if (gather && j0 + kk < len) x[q] = gather_row4<L>(a, Cin, v, gl, pg);
         }
 #pragma unroll
         for (int q = 0; q < kUnroll; q++) {
@@ -654,6 +656,14 @@ cudaError_t GrowB(T **p, int64_t *cap, int64_t need) {
   return e;
 }
 
+// Widest tile whose contrib block has fewer than 2^32 float4 cells (the
+// gather's 32-bit offset): 64 up to 2^26 vertices, 8 for any int32 graph.
+int MaxTileFor(int64_t n) {
+  for (int i = 3; i > 0; i--)
+    if (n * (kTileWidths[i] / 4) <= int64_t(0xffffffffLL)) return kTileWidths[i];
+  return kTileWidths[0];
+}
+
 int PadWidth(int b) {
   for (int w : kTileWidths)
     if (b <= w) return w;
@@ -949,7 +959,8 @@ cudaError_t TuneTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, flo
   std::vector<int32_t> sw(kMaxTile);
   for (int w : kTileWidths) {
     const int B = std::min(w, ncols);
-    if (PadWidth(B) != w) continue;  // would waste a wider tile
+    if (PadWidth(B) != w) continue;     // would waste a wider tile
+    if (w > MaxTileFor(g.n)) continue;  // beyond the gather's 32-bit offsets
     float ms = 0;
     int64_t nl = 0;
     // one warm sweep (graph build), then a timed two-sweep solve
@@ -1018,7 +1029,7 @@ cudaError_t SolveBatched(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s,
     }
     tile = bs.tuned_tile;
   }
-  tile = PadWidth(std::max(1, std::min(tile, kMaxTile)));
+  tile = PadWidth(std::max(1, std::min(std::min(tile, kMaxTile), MaxTileFor(g.n))));
   cudaEvent_t t0, t1;
   PB_TRY(cudaEventCreate(&t0));
   PB_TRY(cudaEventCreate(&t1));
