@@ -16,7 +16,8 @@ PR_GPU_ERANGE = -6
 # Every symbol include/pr_gpu.h declares.
 SYMBOLS = (
     "pr_gpu_create", "pr_gpu_upload", "pr_gpu_upload_sg", "pr_gpu_generate", "pr_gpu_download_csr",
-    "pr_gpu_run", "pr_gpu_run_device",
+    "pr_gpu_run", "pr_gpu_run_device", "pr_gpu_connected_components",
+    "pr_gpu_connected_components_device",
     "pr_gpu_adjoint", "pr_gpu_adjoint_device", "pr_gpu_set_stream",
     "pr_gpu_set_batch_tile", "pr_gpu_get_batch_tile", "pr_gpu_last_timing",
     "pr_gpu_graph_info", "pr_gpu_measure_gather_rate", "pr_gpu_run_noalloc", "pr_gpu_destroy", "pr_gpu_last_error",
@@ -28,6 +29,10 @@ def declare(lib):
     lib.pr_gpu_create.restype = c_int
     lib.pr_gpu_upload.argtypes = [P, c_int64, c_int64, P, P, P, P, P]
     lib.pr_gpu_upload.restype = c_int
+    lib.pr_gpu_connected_components.argtypes = [P, P]
+    lib.pr_gpu_connected_components.restype = c_int
+    lib.pr_gpu_connected_components_device.argtypes = [P, P]
+    lib.pr_gpu_connected_components_device.restype = c_int
     lib.pr_gpu_upload_sg.argtypes = [P, c_char_p]
     lib.pr_gpu_upload_sg.restype = c_int
     lib.pr_gpu_generate.argtypes = [P, c_int, c_int, c_int, P, POINTER(c_int64), POINTER(c_int64)]

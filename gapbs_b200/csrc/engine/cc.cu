@@ -1,0 +1,200 @@
+// cc.cu -- connected components on the device CSR mirror
+// (pr_gpu_connected_components in include/pr_gpu.h).
+//
+// The reference's Afforest (src/cc.cc:40-150) labels every vertex with the
+// root of its component tree; its Link always hooks the larger root under
+// the smaller one and Compress only shortens chains, so every label is at
+// most the vertex's own id and the final root of a component is its
+// smallest vertex id.  That labelling is canonical, and the device computes
+// exactly it:
+//   1. comp[v] = v;
+//   2. two sampling rounds: every vertex links with its r-th out-neighbour
+//      (r = 0, 1), each round followed by a compress;
+//   3. the component of the highest-degree vertex (row 0 of the degree-sorted
+//      mirror: a vertex of the largest intermediate component, which the
+//      reference estimates by sampling) is skipped in the final phase;
+//   4. every other vertex links with its remaining out-neighbours and, for a
+//      directed graph, with all its in-neighbours; compress;
+//   5. ids are mapped back: each root takes the smallest original id of its
+//      component (an atomicMin per vertex), every vertex that root's label.
+// Link is the reference's lock-free hooking loop with compare-and-swap; it
+// and the compress chase are bounded (an iteration limit sets an error flag
+// instead of spinning), so a defect cannot hang the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdint>
+#include <string>
+
+#include "internal.h"
+
+namespace prgpu {
+
+namespace {
+
+constexpr int kChaseLimit = 1 << 20;  // far above any tree depth reached
+
+__device__ __forceinline__ int ld_comp(const int *comp, int x) {
+  return *reinterpret_cast<const volatile int *>(comp + x);
+}
+
+// src/cc.cc:40-55 with compare-and-swap on the device.
+__device__ void cc_link(int u, int v, int *comp, int *err) {
+  int p1 = ld_comp(comp, u);
+  int p2 = ld_comp(comp, v);
+  for (int it = 0; p1 != p2; it++) {
+    if (it >= kChaseLimit) {
+      atomicExch(err, 1);
+      return;
+    }
+    const int high = max(p1, p2), low = min(p1, p2);
+    const int p_high = ld_comp(comp, high);
+    if (p_high == low) return;
+    if (p_high == high && atomicCAS(comp + high, high, low) == high) return;
+    p1 = ld_comp(comp, ld_comp(comp, high));
+    p2 = ld_comp(comp, low);
+  }
+}
+
+__global__ void cc_init_kernel(int32_t n, int *comp) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride)
+    comp[v] = static_cast<int>(v);
+}
+
+// One sampling round: vertex u links with its r-th out-neighbour.
+__global__ void cc_sample_kernel(int32_t n, const int32_t *__restrict__ off,
+                                 const int32_t *__restrict__ nbr, int r, int *comp, int *err) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t u = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u < n; u += stride) {
+    const int s = off[u], e = off[u + 1];
+    if (s + r < e) cc_link(static_cast<int>(u), nbr[s + r], comp, err);
+  }
+}
+
+// src/cc.cc:58-66
+__global__ void cc_compress_kernel(int32_t n, int *comp, int *err) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride) {
+    int it = 0;
+    int c = ld_comp(comp, static_cast<int>(v));
+    int cc = ld_comp(comp, c);
+    while (c != cc) {
+      if (++it >= kChaseLimit) {
+        atomicExch(err, 1);
+        break;
+      }
+      comp[v] = cc;
+      c = cc;
+      cc = ld_comp(comp, c);
+    }
+  }
+}
+
+// Final phase, one warp per vertex: out-neighbours from index `skip` on and,
+// for a directed graph, all in-neighbours; vertices of component `giant` are
+// skipped (src/cc.cc:122-146).
+__global__ void cc_finish_kernel(int32_t n, const int32_t *__restrict__ ooff,
+                                 const int32_t *__restrict__ onbr,
+                                 const int32_t *__restrict__ ioff,
+                                 const int32_t *__restrict__ inbr, int skip, int giant,
+                                 int *comp, int *err) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t u = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; u < n;
+       u += warps) {
+    if (ld_comp(comp, static_cast<int>(u)) == giant) continue;
+    for (int j = ooff[u] + skip + lane; j < ooff[u + 1]; j += 32)
+      cc_link(static_cast<int>(u), onbr[j], comp, err);
+    if (ioff)
+      for (int j = ioff[u] + lane; j < ioff[u + 1]; j += 32)
+        cc_link(static_cast<int>(u), inbr[j], comp, err);
+  }
+}
+
+// Smallest original id of every component, kept at its root.
+__global__ void cc_root_min_kernel(int32_t n, const int *comp, const int32_t *__restrict__ perm,
+                                   int *root_min) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride)
+    atomicMin(root_min + comp[v], perm[v]);
+}
+
+__global__ void cc_label_kernel(int32_t n, const int *comp, const int32_t *__restrict__ perm,
+                                const int *root_min, int32_t *out_old) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride)
+    out_old[perm[v]] = root_min[comp[v]];
+}
+
+__global__ void fill_kernel(int32_t n, int value, int *a) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    a[i] = value;
+}
+
+unsigned CcGrid(int64_t items) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((items + 255) / 256, sms * 16)));
+}
+
+}  // namespace
+
+cudaError_t ConnectedComponents(const DeviceGraph &g, cudaStream_t s, int32_t *out_old,
+                                std::string *err) {
+  const int32_t n = static_cast<int32_t>(g.n);
+  // out-CSR in new ids: the shared CSR of an undirected graph, the
+  // renumbered out-CSR of a directed one
+  const int32_t *ooff = g.directed ? g.orowoff : g.rowoff;
+  const int32_t *onbr = g.directed ? g.ocol : g.col;
+  int *comp = nullptr, *root_min = nullptr, *derr = nullptr;
+  cudaError_t e = cudaMalloc(&comp, sizeof(int) * std::max<int64_t>(n, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&root_min, sizeof(int) * std::max<int64_t>(n, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&derr, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(derr, 0, sizeof(int), s);
+  const unsigned grid = CcGrid(n);
+  const int kRounds = 2;  // neighbor_rounds of src/cc.cc:92
+  if (e == cudaSuccess) {
+    cc_init_kernel<<<grid, 256, 0, s>>>(n, comp);
+    for (int r = 0; r < kRounds; r++) {
+      cc_sample_kernel<<<grid, 256, 0, s>>>(n, ooff, onbr, r, comp, derr);
+      cc_compress_kernel<<<grid, 256, 0, s>>>(n, comp, derr);
+    }
+    e = cudaGetLastError();
+  }
+  int giant = 0;
+  if (e == cudaSuccess && n > 0)
+    e = cudaMemcpyAsync(&giant, comp, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) {
+    const unsigned wgrid = CcGrid(static_cast<int64_t>(n) * 32);
+    cc_finish_kernel<<<wgrid, 256, 0, s>>>(n, ooff, onbr, g.directed ? g.rowoff : nullptr,
+                                           g.directed ? g.col : nullptr, kRounds, giant, comp,
+                                           derr);
+    cc_compress_kernel<<<grid, 256, 0, s>>>(n, comp, derr);
+    fill_kernel<<<grid, 256, 0, s>>>(n, INT_MAX, root_min);
+    cc_root_min_kernel<<<grid, 256, 0, s>>>(n, comp, g.perm, root_min);
+    cc_label_kernel<<<grid, 256, 0, s>>>(n, comp, g.perm, root_min, out_old);
+    e = cudaGetLastError();
+  }
+  int herr = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (comp) cudaFree(comp);
+  if (root_min) cudaFree(root_min);
+  if (derr) cudaFree(derr);
+  if (e != cudaSuccess) {
+    *err = std::string("connected components: ") + cudaGetErrorString(e);
+    return e;
+  }
+  if (herr) {
+    *err = "connected components: link or compress exceeded its iteration limit";
+    return cudaErrorUnknown;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace prgpu

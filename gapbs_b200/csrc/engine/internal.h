@@ -165,6 +165,11 @@ cudaError_t GenerateGraph(bool uniform, int scale, int degree, const int32_t *pe
                           cudaStream_t s, int64_t *n_out, int64_t *m_out, int32_t **off_out,
                           int32_t **nbr_out, std::string *err);
 void WidenOffsets(int64_t n1, const int32_t *off32, int64_t *off64, cudaStream_t s);
+
+// Connected components of the uploaded graph (cc.cu): out_old[v] = the
+// smallest original vertex id of v's component (device buffer, n entries).
+cudaError_t ConnectedComponents(const DeviceGraph &g, cudaStream_t s, int32_t *out_old,
+                                std::string *err);
 // int64 CSR offsets -> int32, setting *bad for values outside [0, 2^31).
 void NarrowOffsets(int64_t count, const int64_t *wide, int32_t *narrow, int *bad, cudaStream_t s);
 

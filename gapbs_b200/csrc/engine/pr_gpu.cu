@@ -626,6 +626,30 @@ int pr_gpu_upload_sg(pr_gpu_t *h, const char *path) {
   return PR_GPU_OK;
 }
 
+int pr_gpu_connected_components_device(pr_gpu_t *h, int32_t *comp_out_dev) {
+  if (!h) return PR_GPU_EINVAL;
+  if (!h->has_graph) return SetErr(h, PR_GPU_ENOGRAPH, "no graph uploaded");
+  if (!comp_out_dev) return SetErr(h, PR_GPU_EINVAL, "comp_out is null");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  std::string msg;
+  cudaError_t e = prgpu::ConnectedComponents(h->g, h->stream, comp_out_dev, &msg);
+  if (e != cudaSuccess) return SetErr(h, PR_GPU_ECUDA, msg);
+  return PR_GPU_OK;
+}
+
+int pr_gpu_connected_components(pr_gpu_t *h, int32_t *comp_out) {
+  if (!h) return PR_GPU_EINVAL;
+  if (!h->has_graph) return SetErr(h, PR_GPU_ENOGRAPH, "no graph uploaded");
+  if (!comp_out) return SetErr(h, PR_GPU_EINVAL, "comp_out is null");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  int32_t *d = nullptr;
+  PR_CHECK(h, cudaMalloc(&d, sizeof(int32_t) * h->g.n));
+  int rc = pr_gpu_connected_components_device(h, d);
+  if (!rc) rc = CopyToHost(h, comp_out, d, sizeof(int32_t) * h->g.n);
+  cudaFree(d);
+  return rc;
+}
+
 int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m, const int32_t *out_off,
                   const int32_t *out_nbr, const int32_t *in_off, const int32_t *in_nbr,
                   const float *edge_w) {

@@ -7,7 +7,8 @@
 // "i:t:"): -f file, -g/-u scale, -k degree, -s, -m, -a, -n trials, -r node,
 // -v, -l, -i max iterations, -t tolerance, -h.  "-g10 -vn1" style bundles
 // parse as getopt parses them.  Unknown letters are reported and skipped,
-// as getopt does.
+// as getopt does.  Built with iterative = false it is the reference's plain
+// CLApp (no -i / -t), the command line of its cc binary.
 #ifndef GAPBS_B200_HOST_COMMAND_LINE_H_
 #define GAPBS_B200_HOST_COMMAND_LINE_H_
 
@@ -23,8 +24,8 @@ namespace gapbs_b200 {
 
 class PageRankCLI {
  public:
-  PageRankCLI(std::string name, double tolerance, int max_iters)
-      : name_(name), tolerance_(tolerance), max_iters_(max_iters) {
+  PageRankCLI(std::string name, double tolerance, int max_iters, bool iterative = true)
+      : name_(name), tolerance_(tolerance), max_iters_(max_iters), iterative_(iterative) {
     Help('h', "", "print this help message");
     Help('f', "file", "load graph from file");
     Help('s', "", "symmetrize input edge list", "false");
@@ -37,14 +38,16 @@ class PageRankCLI {
     Help('r', "node", "start from node r", "rand");
     Help('v', "", "verify the output of each run", "false");
     Help('l', "", "log performance within each trial", "false");
-    Help('i', "i", "perform at most i iterations", std::to_string(max_iters_));
-    Help('t', "t", "use tolerance t", std::to_string(tolerance_));
+    if (iterative_) {
+      Help('i', "i", "perform at most i iterations", std::to_string(max_iters_));
+      Help('t', "t", "use tolerance t", std::to_string(tolerance_));
+    }
   }
 
   // Returns false (after printing the reference's message) when no graph
   // input was given.  -h prints usage and exits 0, as the reference does.
   bool Parse(int argc, char **argv) {
-    const std::string with_arg = "fgkunrit";
+    const std::string with_arg = iterative_ ? "fgkunrit" : "fgkunr";
     const std::string flags = "hsmavl";
     for (int i = 1; i < argc; i++) {
       const char *tok = argv[i];
@@ -131,6 +134,7 @@ class PageRankCLI {
   bool logging_ = false;
   double tolerance_;
   int max_iters_;
+  bool iterative_;
   std::vector<std::string> help_;
 };
 

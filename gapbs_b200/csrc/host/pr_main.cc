@@ -18,6 +18,7 @@
 #include "benchmark.h"
 #include "builder.h"
 #include "command_line.h"
+#include "device_graph.h"
 #include "graph.h"
 #include "pr_gpu.h"
 #include "util.h"
@@ -30,65 +31,6 @@ static const float kDamp = 0.85f;  // src/pr_spmv.cc:33
 namespace {
 
 pr_gpu_t *g_engine = nullptr;
-
-[[noreturn]] void Die(int code, const std::string &msg) {
-  std::cout << msg << std::endl;
-  std::exit(code);
-}
-
-// One-time upload of the CSR (int32 offsets) to device 0.
-void UploadGraph(const HostGraph &g) {
-  WallTimer t;
-  t.Start();
-  int rc = pr_gpu_create(&g_engine, 0);
-  if (rc) Die(rc, "pr_gpu_create failed: no usable CUDA device");
-  const int64_t n = g.num_nodes();
-  const int64_t m = g.out_entries();
-  if (m > 0x7fffffffLL - 8) Die(PR_GPU_ERANGE, "graph exceeds int32 offsets");
-  std::vector<int32_t> out_off(n + 1), in_off;
-  for (int64_t i = 0; i <= n; i++) out_off[i] = static_cast<int32_t>(g.out_off_ptr()[i]);
-  if (g.directed()) {
-    in_off.resize(n + 1);
-    for (int64_t i = 0; i <= n; i++) in_off[i] = static_cast<int32_t>(g.in_off_ptr()[i]);
-  }
-  rc = pr_gpu_upload(g_engine, n, m, out_off.data(), g.out_nbr_ptr(),
-                     g.directed() ? in_off.data() : nullptr,
-                     g.directed() ? g.in_nbr_ptr() : nullptr, nullptr);
-  if (rc) Die(rc, std::string("pr_gpu_upload failed: ") + pr_gpu_last_error(g_engine));
-  t.Stop();
-  PrintTime("Upload Time", t.Seconds());
-}
-
-// -g / -u on the device: the reference's graph, uploaded as it is built.
-// Returns false (host path) for sizes the device path does not cover.
-bool GenerateOnDevice(const GraphSource &src, HostGraph *g) {
-  if (src.scale < 1 || src.scale > 30 || src.degree < 0) return false;
-  if ((int64_t(2) * src.degree) << src.scale > 0x7fffffffLL - 8) return false;
-  WallTimer t;
-  t.Start();
-  int rc = pr_gpu_create(&g_engine, 0);
-  if (rc) Die(rc, "pr_gpu_create failed: no usable CUDA device");
-  std::vector<NodeID> perm;
-  if (!src.uniform) {
-    perm.resize(size_t(1) << src.scale);
-    RMatPermutation(src.scale, perm.data());
-  }
-  int64_t n = 0, m = 0;
-  rc = pr_gpu_generate(g_engine, src.uniform ? 1 : 0, src.scale, src.degree,
-                       src.uniform ? nullptr : perm.data(), &n, &m);
-  if (rc) Die(rc, std::string("pr_gpu_generate failed: ") + pr_gpu_last_error(g_engine));
-  t.Stop();
-  PrintTime("Generate Time", t.Seconds());
-  t.Start();
-  Buffer<Offset> off(static_cast<size_t>(n + 1));
-  Buffer<NodeID> nbr(static_cast<size_t>(m > 0 ? m : 1));
-  rc = pr_gpu_download_csr(g_engine, off.data(), nbr.data());
-  if (rc) Die(rc, std::string("pr_gpu_download_csr failed: ") + pr_gpu_last_error(g_engine));
-  *g = HostGraph::Undirected(n, std::move(off), std::move(nbr));
-  t.Stop();
-  PrintTime("Build Time", t.Seconds());
-  return true;
-}
 
 // src/pr_spmv.cc:35-61, computed by the engine.
 std::vector<ScoreT> PageRankPull(const HostGraph &g, int max_iters, double epsilon = 0,
@@ -132,15 +74,7 @@ bool PRVerifier(const HostGraph &g, const std::vector<ScoreT> &scores, double ta
 int main(int argc, char *argv[]) {
   PageRankCLI cli("pagerank", 1e-4, 20);
   if (!cli.Parse(argc, argv)) return -1;
-  HostGraph g;
-  if (!GenerateOnDevice(cli.source(), &g)) {
-    try {
-      g = MakeGraph(cli.source(), true);
-    } catch (const BuildError &e) {
-      Die(e.code(), e.what());
-    }
-    UploadGraph(g);
-  }
+  HostGraph g = AcquireGraph(cli.source(), &g_engine);
   auto PRBound = [&cli](const HostGraph &graph) {
     return PageRankPull(graph, cli.max_iters(), cli.tolerance(), cli.logging_en());
   };

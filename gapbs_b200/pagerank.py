@@ -110,6 +110,14 @@ class PageRankEngine:
         else:
             self.upload_csr(g.num_nodes, g.out_offsets, g.out_neighbors, None, None, edge_w)
 
+    def connected_components(self) -> np.ndarray:
+        """Component label of every vertex of the uploaded graph: the smallest
+        vertex id of its component (the reference's Afforest labelling)."""
+        comp = np.empty(self.n, np.int32)
+        self._check(self._lib.pr_gpu_connected_components(self._h, _ptr(comp)),
+                    "pr_gpu_connected_components")
+        return comp
+
     def upload_sg(self, path: str):
         """Uploads a serialized (.sg) graph file straight to the device (no host
         CSR); returns (num_nodes, CSR entries)."""

@@ -99,6 +99,15 @@ int pr_gpu_generate(pr_gpu_t *h, int uniform, int scale, int degree,
  * offsets, m_out neighbours), then frees the device copy. */
 int pr_gpu_download_csr(pr_gpu_t *h, int64_t *out_off, int32_t *out_nbr);
 
+/* Connected components of the uploaded graph, the reference's Afforest
+ * (src/cc.cc:40-150: two neighbour-sampling rounds, the largest
+ * intermediate component skipped in the final link phase, a directed graph
+ * linked through its in-neighbours too).  comp_out[v] (n entries, original
+ * ids) = the smallest vertex id of v's component, which is the label the
+ * reference's Link/Compress produce.  Host buffer / device buffer forms. */
+int pr_gpu_connected_components(pr_gpu_t *h, int32_t *comp_out);
+int pr_gpu_connected_components_device(pr_gpu_t *h, int32_t *comp_out_dev);
+
 /* Runs Jacobi PageRank sweeps until the L1 change of a sweep is < epsilon or
  * max_iters sweeps have run (src/pr_spmv.cc:41-58).
  *

@@ -45,6 +45,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_pr_verify_f32.restype = c_double
         L.oracle_pr_residual_f64.argtypes = [c_int64, P, P, P, c_float, P]
         L.oracle_pr_residual_f64.restype = c_double
+        L.oracle_cc_afforest.argtypes = [c_int64, P, P, P, P, c_int, P]
+        L.oracle_cc_afforest.restype = None
         L.oracle_ppr_residual_f64.argtypes = [c_int64, P, P, P, c_float, P, P]
         L.oracle_ppr_residual_f64.restype = c_double
         L.oracle_ppr_f64.argtypes = [c_int64, P, P, P, P, P, c_double, P, c_int, c_double, P, P]
@@ -97,6 +99,40 @@ def pr_residual_f64(g, scores, damping=0.85) -> float:
     n, io, inb, oo, _ = _csr(g)
     s = np.ascontiguousarray(scores, np.float32)
     return float(lib().oracle_pr_residual_f64(n, _ptr(io), _ptr(inb), _ptr(oo), damping, _ptr(s)))
+
+
+def cc_afforest(g) -> np.ndarray:
+    """Component labels by the serial restatement of the reference's Afforest."""
+    n = g.num_nodes
+    oo = np.ascontiguousarray(g.out_offsets, np.int64)
+    on = np.ascontiguousarray(g.out_neighbors, np.int32)
+    io = np.ascontiguousarray(g.in_offsets, np.int64)
+    inb = np.ascontiguousarray(g.in_neighbors, np.int32)
+    comp = np.empty(n, np.int32)
+    lib().oracle_cc_afforest(n, _ptr(oo), _ptr(on), _ptr(io), _ptr(inb), int(g.directed),
+                             _ptr(comp))
+    return comp
+
+
+def ref_cc_afforest(args: str):
+    """The reference's own Afforest on the graph its builder makes for args
+    (pr_spmv-style options).  Returns (labels, kernel seconds)."""
+    path = os.path.join(REF_DIR, "libgapbs_ref_cc.so")
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} missing (built by `make -C oracle` where the reference "
+                           "tree exists)")
+    R = ctypes.CDLL(path)
+    R.ref_cc_afforest.argtypes = [c_int, POINTER(c_char_p), P, c_int64, POINTER(c_double)]
+    R.ref_cc_afforest.restype = c_int64
+    toks = ["cc"] + args.split()
+    argv = (c_char_p * len(toks))(*[t.encode() for t in toks])
+    sec = c_double()
+    n = R.ref_cc_afforest(len(toks), argv, None, 0, ctypes.byref(sec))
+    if n < 0:
+        raise RuntimeError(f"reference rejected {args!r}")
+    comp = np.empty(n, np.int32)
+    R.ref_cc_afforest(len(toks), argv, _ptr(comp), n, ctypes.byref(sec))
+    return comp, float(sec.value)
 
 
 def ppr_residual_f64(g, t, s, damping=0.85) -> float:

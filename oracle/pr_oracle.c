@@ -228,3 +228,64 @@ int oracle_ppr_adjoint_f64(int64_t n, const int64_t *out_off,
   free(plam);
   return sweeps;
 }
+
+/* ---- connected components (src/cc.cc) ---------------------------------- */
+
+/* :40-55, serial: hook the larger root under the smaller one. */
+static void cc_link(int32_t u, int32_t v, int32_t *comp) {
+  int32_t p1 = comp[u], p2 = comp[v];
+  while (p1 != p2) {
+    int32_t high = p1 > p2 ? p1 : p2;
+    int32_t low = p1 + (p2 - high);
+    int32_t p_high = comp[high];
+    if (p_high == low) break;
+    if (p_high == high) {
+      comp[high] = low;
+      break;
+    }
+    p1 = comp[comp[high]];
+    p2 = comp[low];
+  }
+}
+
+/* :58-66 */
+static void cc_compress(int64_t n, int32_t *comp) {
+  for (int64_t v = 0; v < n; v++)
+    while (comp[v] != comp[comp[v]]) comp[v] = comp[comp[v]];
+}
+
+void oracle_cc_afforest(int64_t n, const int64_t *out_off, const int32_t *out_nbr,
+                        const int64_t *in_off, const int32_t *in_nbr, int directed,
+                        int32_t *comp) {
+  const int rounds = 2; /* :92 */
+  for (int64_t v = 0; v < n; v++) comp[v] = (int32_t)v;
+  for (int r = 0; r < rounds; r++) { /* :100-110 */
+    for (int64_t u = 0; u < n; u++)
+      if (out_off[u] + r < out_off[u + 1]) cc_link((int32_t)u, out_nbr[out_off[u] + r], comp);
+    cc_compress(n, comp);
+  }
+  /* :69-87: the most frequent label among a sample; the final labels do not
+   * depend on which component is skipped, so a fixed stride sample serves */
+  int32_t giant = 0;
+  if (n > 0) {
+    int64_t best = 0;
+    const int64_t step = n > 1024 ? n / 1024 : 1;
+    for (int64_t a = 0; a < n; a += step) {
+      int64_t count = 0;
+      for (int64_t b = 0; b < n; b += step)
+        if (comp[b] == comp[a]) count++;
+      if (count > best) {
+        best = count;
+        giant = comp[a];
+      }
+    }
+  }
+  for (int64_t u = 0; u < n; u++) { /* :116-146 */
+    if (comp[u] == giant) continue;
+    for (int64_t e = out_off[u] + rounds; e < out_off[u + 1]; e++)
+      cc_link((int32_t)u, out_nbr[e], comp);
+    if (directed)
+      for (int64_t e = in_off[u]; e < in_off[u + 1]; e++) cc_link((int32_t)u, in_nbr[e], comp);
+  }
+  cc_compress(n, comp);
+}

@@ -97,6 +97,16 @@ int oracle_ppr_adjoint_f64(int64_t n, const int64_t *out_off,
                            const double *s, int max_iters, double epsilon,
                            double *lambda, double *grad_t, double *grad_ew);
 
+/* Connected components, the reference's Afforest (src/cc.cc:40-150) run
+ * serially: two sampling rounds linking each vertex with its r-th
+ * out-neighbour, compress, then every vertex outside the largest sampled
+ * component links with its remaining out-neighbours (and, when directed,
+ * all in-neighbours), compress.  comp[v] = the smallest vertex id of v's
+ * component, as the reference's Link/Compress leave it. */
+void oracle_cc_afforest(int64_t n, const int64_t *out_off, const int32_t *out_nbr,
+                        const int64_t *in_off, const int32_t *in_nbr, int directed,
+                        int32_t *comp);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,7 +28,13 @@ from its own sources by oracle/Makefile) exist.  Writes:
                                      invocations (missing file, unknown
                                      suffix, missing or unknown option)
 
-Usage:  python tests/golden/make_golden.py [--fullsize | --cli]
+  cc_golden.json                     (--cc) the reference's Afforest connected
+                                     components on small and mid-size graphs:
+                                     component count, sha256 of the int32
+                                     labels, the labels themselves for the
+                                     smallest graphs
+
+Usage:  python tests/golden/make_golden.py [--fullsize | --cli | --cc]
 """
 from __future__ import annotations
 
@@ -244,21 +250,62 @@ def main_fullsize():
 CLI_CASES = ["-h", "-f {tmp}/missing.el", "-f {tmp}/x.foo", "-g", "-z", "-n"]
 
 
+# cc -a runs whose analysis lines (clusters, component count) are recorded
+CC_ANALYSIS_CASES = ["-g 10 -n 1 -a", "-u 12 -k 1 -n 1 -a", "-f {graphs}/4.el -n 1 -a"]
+
+
 def main_cli():
     import subprocess
-    exe = os.path.join(ROOT, "oracle", "_ref", "pr_spmv")
-    if not os.path.exists(exe):
-        sys.exit("needs oracle/_ref/pr_spmv (make -C oracle where the reference tree exists)")
-    out = {"generator": "tests/golden/make_golden.py --cli", "cases": []}
+    out = {"generator": "tests/golden/make_golden.py --cli", "cases": [], "cc_analysis": []}
     with tempfile.TemporaryDirectory() as tmp:
         open(os.path.join(tmp, "x.foo"), "w").close()
-        for args in CLI_CASES:
-            p = subprocess.run([exe] + args.format(tmp=tmp).split(), capture_output=True, text=True)
-            out["cases"].append({"args": args, "returncode": p.returncode,
-                                 "stdout": p.stdout.replace(tmp, "{tmp}")})
-            print(args, p.returncode)
+        for binary in ("pr_spmv", "cc"):
+            exe = os.path.join(ROOT, "oracle", "_ref", binary)
+            if not os.path.exists(exe):
+                sys.exit(f"needs oracle/_ref/{binary} (make -C oracle where the reference tree exists)")
+            for args in CLI_CASES:
+                p = subprocess.run([exe] + args.format(tmp=tmp).split(), capture_output=True,
+                                   text=True)
+                out["cases"].append({"binary": binary, "args": args, "returncode": p.returncode,
+                                     "stdout": p.stdout.replace(tmp, "{tmp}")})
+                print(binary, args, p.returncode)
+    gdir = os.path.join(HERE, "graphs")
+    exe = os.path.join(ROOT, "oracle", "_ref", "cc")
+    for args in CC_ANALYSIS_CASES:
+        p = subprocess.run([exe] + args.format(graphs=gdir).split(), capture_output=True, text=True)
+        lines = p.stdout.splitlines()
+        i = next(k for k, ln in enumerate(lines) if ln.endswith("biggest clusters"))
+        j = next(k for k, ln in enumerate(lines) if ln.startswith("There are "))
+        out["cc_analysis"].append({"args": args, "lines": lines[i - 1:j + 1]})
+        print("cc", args, lines[j])
     with open(os.path.join(HERE, "cli_golden.json"), "w") as fh:
         json.dump(out, fh, indent=1)
+
+
+# (case name, options, keep the label array)
+CC_CASES = [
+    ("g10", "-g 10", True), ("u10", "-u 10", True), ("g12k2", "-g 12 -k 2", True),
+    ("u12k1", "-u 12 -k 1", True), ("g14k2", "-g 14 -k 2", False), ("g16", "-g 16", False),
+    ("g18k4", "-g 18 -k 4", False), ("u18k1", "-u 18 -k 1", False),
+    ("el4", "-f {graphs}/4.el", True), ("el4s", "-f {graphs}/4.el -s", True),
+    ("mtx4", "-f {graphs}/4.mtx", True), ("gr4", "-f {graphs}/4.gr", True),
+]
+
+
+def main_cc():
+    gdir = os.path.join(HERE, "graphs")
+    out = {"generator": "tests/golden/make_golden.py --cc", "cases": {}}
+    for name, args, keep in CC_CASES:
+        a = args.format(graphs=gdir)
+        (comp, _), _ = capture_stdout(oracle.ref_cc_afforest, a)
+        entry = {"args": args, "num_nodes": int(comp.size),
+                 "components": int(np.unique(comp).size), "labels_sha256": sha(comp)}
+        if keep:
+            entry["labels"] = [int(x) for x in comp]
+        out["cases"][name] = entry
+        print(name, comp.size, entry["components"])
+    with open(os.path.join(HERE, "cc_golden.json"), "w") as fh:
+        json.dump(out, fh, separators=(",", ":"))
 
 
 if __name__ == "__main__":
@@ -266,6 +313,9 @@ if __name__ == "__main__":
         main_fullsize()
     elif "--cli" in sys.argv[1:]:
         main_cli()
+    elif "--cc" in sys.argv[1:]:
+        main_cc()
     else:
         main()
         main_cli()
+        main_cc()

@@ -1,5 +1,6 @@
-"""pr_gpu end to end on the GPU, the way the reference's test/test.mk runs
-pr_spmv: the verification line, the -l step lines and the -a top scores.
+"""pr_gpu and cc_gpu end to end on the GPU, the way the reference's
+test/test.mk runs pr_spmv and cc: the verification line, the -l step lines,
+the -a top scores of PageRank and the -a cluster lines of CC.
 """
 import json
 import os
@@ -12,6 +13,9 @@ from conftest import GOLDEN, ROOT, gpu_available
 
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(ROOT, "gapbs_b200", "bin", "pr_gpu")
+CC_EXE = os.path.join(ROOT, "gapbs_b200", "bin", "cc_gpu")
+with open(os.path.join(GOLDEN, "cli_golden.json")) as fh:
+    CC_ANALYSIS = json.load(fh)["cc_analysis"]
 with open(os.path.join(GOLDEN, "pr_golden.json")) as fh:
     GOLD = json.load(fh)["cases"]
 STEP = re.compile(r"^ {4}\d+ +\d+\.\d{5}$")
@@ -53,3 +57,20 @@ def test_log_lines_and_top_scores(exe):
     assert [int(t.group(1)) for t in top] == [v for v, _ in e["top5"]]
     for t, (_, sc) in zip(top, e["top5"]):
         assert abs(float(t.group(2)) - sc) <= 1e-5 * sc
+
+
+@pytest.mark.parametrize("case", CC_ANALYSIS, ids=[c["args"] for c in CC_ANALYSIS])
+def test_cc_analysis_and_verification(exe, case):
+    args = case["args"].format(graphs=os.path.join(GOLDEN, "graphs")).split() + ["-v"]
+    out = run(CC_EXE, args)
+    lines = out.splitlines()
+    i = next(k for k, ln in enumerate(lines) if ln.endswith("biggest clusters"))
+    j = next(k for k, ln in enumerate(lines) if ln.startswith("There are "))
+    assert lines[i - 1:j + 1] == case["lines"]
+    assert "Verification:           PASS" in out
+
+
+def test_cc_verification_on_larger_graphs(exe):
+    for args in ("-g 16 -n 2 -v", "-u 16 -k 2 -n 1 -v"):
+        out = run(CC_EXE, args.split())
+        assert out.count("Verification:           PASS") == int(args.split()[args.split().index("-n") + 1])
