@@ -57,6 +57,7 @@ def parse_args():
     p.add_argument("--no-ppr", action="store_true")
     p.add_argument("--adjoint-graph", default="-g 20")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-cc", action="store_true")
     p.add_argument("--e2e-upload-steps", type=int, default=3,
                    help="steps of the end-to-end variant that uploads the graph every step")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -335,6 +336,27 @@ def run_ours(a, dist: Dist):
     e2e_edges = dist.sum(float(m) * e2e_sweeps)
     e2e_value = e2e_edges / e2e_s / 1e9
 
+    # ---- connected components (the reference's Afforest) on the same graph
+    cc = None
+    if not a.no_cc:
+        comp = torch.empty(n, dtype=torch.int32, device=f"cuda:{dev}")
+        eng.set_stream(stream.cuda_stream)
+        for _ in range(max(1, a.warmup)):
+            eng.connected_components_device(comp.data_ptr())
+        torch.cuda.synchronize()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(a.steps):
+            eng.connected_components_device(comp.data_ptr())
+        c1.record(stream)
+        torch.cuda.synchronize()
+        cc_ms = dist.max(c0.elapsed_time(c1) / a.steps)
+        cc = {"workload": f"Afforest connected components of {a.graph.strip()}",
+              "ms": round(cc_ms, 3), "unit": "ms per run (device-resident graph)",
+              "edges_per_s": round(m / (cc_ms / 1e3) / 1e9, 2),
+              "components": int(torch.unique(comp).numel())}
+        eng.set_stream(None)
+
     # ---- end to end with the graph uploaded every step (a caller whose graph
     # changes between solves): pr_gpu_upload of the host CSR + pr_gpu_run
     e2e_up = None
@@ -430,6 +452,8 @@ def run_ours(a, dist: Dist):
     }
     if e2e_up is not None:
         result["e2e_graph_upload_each_step"] = e2e_up
+    if cc is not None:
+        result["cc"] = cc
     del flush
 
     # ---- batched PPR vs sequential single-vector solves (rank 0, N=1 config)
@@ -443,6 +467,13 @@ def run_ours(a, dist: Dist):
         if g is None:
             g = eng.download_graph()  # the generated graph, for the reference on the host
         result["cpu_baseline"] = cpu_baseline(g, a, sweeps_per_step)
+        if cc is not None:
+            import oracle
+            if oracle.ref_available():
+                _, sec = oracle.ref_cc_afforest_csr(g, trials=2)
+                cc["reference_cpu_ms"] = round(sec * 1e3, 3)
+                cc["reference_cpu_cores"] = os.cpu_count() or 1
+                cc["speedup_vs_reference_cpu"] = round(sec * 1e3 / cc["ms"], 2)
     eng.close()
     return result
 

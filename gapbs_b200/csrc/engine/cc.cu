@@ -12,11 +12,14 @@
 //      (r = 0, 1), each round followed by a compress;
 //   3. the component of the highest-degree vertex (row 0 of the degree-sorted
 //      mirror: a vertex of the largest intermediate component, which the
-//      reference estimates by sampling) is skipped in the final phase;
+//      reference estimates by sampling) is skipped in the final phase; row 0
+//      has the smallest id, so it is the root of its tree and that
+//      component's label is 0;
 //   4. every other vertex links with its remaining out-neighbours and, for a
 //      directed graph, with all its in-neighbours; compress;
 //   5. ids are mapped back: each root takes the smallest original id of its
-//      component (an atomicMin per vertex), every vertex that root's label.
+//      component (atomicMin; the largest component's members reduced per
+//      block first), every vertex that root's label.
 // Link is the reference's lock-free hooking loop with compare-and-swap; it
 // and the compress chase are bounded (an iteration limit sets an error flag
 // instead of spinning), so a defect cannot hang the device.
@@ -113,12 +116,30 @@ __global__ void cc_finish_kernel(int32_t n, const int32_t *__restrict__ ooff,
   }
 }
 
-// Smallest original id of every component, kept at its root.
-__global__ void cc_root_min_kernel(int32_t n, const int *comp, const int32_t *__restrict__ perm,
-                                   int *root_min) {
+// Smallest original id of every component, kept at its root.  Members of
+// the component of row 0 (the largest one; half the graph on Kronecker
+// inputs) are reduced per thread and per block first, so its root takes one
+// atomic per block instead of one per vertex.
+__global__ void __launch_bounds__(256) cc_root_min_kernel(int32_t n, const int *comp,
+                                                          const int32_t *__restrict__ perm,
+                                                          int *root_min) {
+  __shared__ int s_min[8];
+  const int giant = 0;  // row 0 is the root of its component
+  int local = INT_MAX;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride)
-    atomicMin(root_min + comp[v], perm[v]);
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride) {
+    const int c = comp[v];
+    if (c == giant) local = min(local, perm[v]);
+    else atomicMin(root_min + c, perm[v]);
+  }
+  local = static_cast<int>(__reduce_min_sync(0xffffffffu, static_cast<unsigned>(local)));
+  if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = local;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int m = INT_MAX;
+    for (int w = 0; w < (blockDim.x >> 5); w++) m = min(m, s_min[w]);
+    if (m != INT_MAX) atomicMin(root_min + giant, m);
+  }
 }
 
 __global__ void cc_label_kernel(int32_t n, const int *comp, const int32_t *__restrict__ perm,
@@ -143,18 +164,35 @@ unsigned CcGrid(int64_t items) {
 
 }  // namespace
 
-cudaError_t ConnectedComponents(const DeviceGraph &g, cudaStream_t s, int32_t *out_old,
-                                std::string *err) {
+void FreeCcScratch(CcScratch *c) {
+  for (int *p : {c->comp, c->root_min, c->err})
+    if (p) cudaFree(p);
+  c->comp = c->root_min = c->err = nullptr;
+  c->cap = 0;
+}
+
+cudaError_t ConnectedComponents(const DeviceGraph &g, CcScratch &cs, cudaStream_t s,
+                                int32_t *out_old, std::string *err) {
   const int32_t n = static_cast<int32_t>(g.n);
   // out-CSR in new ids: the shared CSR of an undirected graph, the
   // renumbered out-CSR of a directed one
   const int32_t *ooff = g.directed ? g.orowoff : g.rowoff;
   const int32_t *onbr = g.directed ? g.ocol : g.col;
-  int *comp = nullptr, *root_min = nullptr, *derr = nullptr;
-  cudaError_t e = cudaMalloc(&comp, sizeof(int) * std::max<int64_t>(n, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&root_min, sizeof(int) * std::max<int64_t>(n, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&derr, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemsetAsync(derr, 0, sizeof(int), s);
+  cudaError_t e = cudaSuccess;
+  if (!cs.comp || cs.cap < n) {
+    FreeCcScratch(&cs);
+    e = cudaMalloc(&cs.comp, sizeof(int) * std::max<int64_t>(n, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&cs.root_min, sizeof(int) * std::max<int64_t>(n, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&cs.err, sizeof(int));
+    if (e != cudaSuccess) {
+      FreeCcScratch(&cs);
+      *err = std::string("connected components: ") + cudaGetErrorString(e);
+      return e;
+    }
+    cs.cap = n;
+  }
+  int *comp = cs.comp, *root_min = cs.root_min, *derr = cs.err;
+  e = cudaMemsetAsync(derr, 0, sizeof(int), s);
   const unsigned grid = CcGrid(n);
   const int kRounds = 2;  // neighbor_rounds of src/cc.cc:92
   if (e == cudaSuccess) {
@@ -165,10 +203,7 @@ cudaError_t ConnectedComponents(const DeviceGraph &g, cudaStream_t s, int32_t *o
     }
     e = cudaGetLastError();
   }
-  int giant = 0;
-  if (e == cudaSuccess && n > 0)
-    e = cudaMemcpyAsync(&giant, comp, sizeof(int), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  const int giant = 0;  // the root, and label, of row 0's component
   if (e == cudaSuccess) {
     const unsigned wgrid = CcGrid(static_cast<int64_t>(n) * 32);
     cc_finish_kernel<<<wgrid, 256, 0, s>>>(n, ooff, onbr, g.directed ? g.rowoff : nullptr,
@@ -183,9 +218,6 @@ cudaError_t ConnectedComponents(const DeviceGraph &g, cudaStream_t s, int32_t *o
   int herr = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (comp) cudaFree(comp);
-  if (root_min) cudaFree(root_min);
-  if (derr) cudaFree(derr);
   if (e != cudaSuccess) {
     *err = std::string("connected components: ") + cudaGetErrorString(e);
     return e;

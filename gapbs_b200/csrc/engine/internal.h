@@ -168,8 +168,13 @@ void WidenOffsets(int64_t n1, const int32_t *off32, int64_t *off64, cudaStream_t
 
 // Connected components of the uploaded graph (cc.cu): out_old[v] = the
 // smallest original vertex id of v's component (device buffer, n entries).
-cudaError_t ConnectedComponents(const DeviceGraph &g, cudaStream_t s, int32_t *out_old,
-                                std::string *err);
+struct CcScratch {
+  int *comp = nullptr, *root_min = nullptr, *err = nullptr;
+  int64_t cap = 0;
+};
+void FreeCcScratch(CcScratch *c);
+cudaError_t ConnectedComponents(const DeviceGraph &g, CcScratch &cs, cudaStream_t s,
+                                int32_t *out_old, std::string *err);
 // int64 CSR offsets -> int32, setting *bad for values outside [0, 2^31).
 void NarrowOffsets(int64_t count, const int64_t *wide, int32_t *narrow, int *bad, cudaStream_t s);
 

@@ -40,6 +40,7 @@ struct pr_gpu {
   // CSR of the last pr_gpu_generate (original ids), kept for download
   int32_t *gen_off = nullptr, *gen_nbr = nullptr;
   int64_t gen_n = 0, gen_m = 0;
+  prgpu::CcScratch cc;  // connected-components work arrays
 };
 
 namespace {
@@ -442,6 +443,7 @@ void pr_gpu_destroy(pr_gpu_t *h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   FreeGenerated(h);
+  prgpu::FreeCcScratch(&h->cc);
   h->loop_single.Reset();
   h->loop_adjoint.Reset();
   prgpu::FreeDeviceGraph(&h->g);
@@ -632,7 +634,7 @@ int pr_gpu_connected_components_device(pr_gpu_t *h, int32_t *comp_out_dev) {
   if (!comp_out_dev) return SetErr(h, PR_GPU_EINVAL, "comp_out is null");
   PR_CHECK(h, cudaSetDevice(h->device));
   std::string msg;
-  cudaError_t e = prgpu::ConnectedComponents(h->g, h->stream, comp_out_dev, &msg);
+  cudaError_t e = prgpu::ConnectedComponents(h->g, h->cc, h->stream, comp_out_dev, &msg);
   if (e != cudaSuccess) return SetErr(h, PR_GPU_ECUDA, msg);
   return PR_GPU_OK;
 }

@@ -118,6 +118,11 @@ class PageRankEngine:
                     "pr_gpu_connected_components")
         return comp
 
+    def connected_components_device(self, comp_ptr: int):
+        """Component labels into a device buffer of n int32 (on the handle's GPU)."""
+        self._check(self._lib.pr_gpu_connected_components_device(self._h, comp_ptr),
+                    "pr_gpu_connected_components_device")
+
     def upload_sg(self, path: str):
         """Uploads a serialized (.sg) graph file straight to the device (no host
         CSR); returns (num_nodes, CSR entries)."""

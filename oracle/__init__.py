@@ -135,6 +135,26 @@ def ref_cc_afforest(args: str):
     return comp, float(sec.value)
 
 
+def ref_cc_afforest_csr(g, trials: int = 1):
+    """The reference's Afforest on graph g's CSR.  Returns (labels, fastest
+    kernel seconds over `trials` runs)."""
+    path = os.path.join(REF_DIR, "libgapbs_ref_cc.so")
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} missing (built by `make -C oracle` where the reference "
+                           "tree exists)")
+    R = ctypes.CDLL(path)
+    R.ref_cc_afforest_csr.argtypes = [c_int64, c_int, P, P, P, P, c_int, P]
+    R.ref_cc_afforest_csr.restype = c_double
+    oo = np.ascontiguousarray(g.out_offsets, np.int64)
+    on = np.ascontiguousarray(g.out_neighbors, np.int32)
+    io = np.ascontiguousarray(g.in_offsets, np.int64)
+    inb = np.ascontiguousarray(g.in_neighbors, np.int32)
+    comp = np.empty(g.num_nodes, np.int32)
+    sec = R.ref_cc_afforest_csr(g.num_nodes, int(g.directed), _ptr(oo), _ptr(on), _ptr(io),
+                                _ptr(inb), int(trials), _ptr(comp))
+    return comp, float(sec)
+
+
 def ppr_residual_f64(g, t, s, damping=0.85) -> float:
     """L1 residual of one PPR score column (unit weights); see pr_oracle.h."""
     n, io, inb, oo, _ = _csr(g)
