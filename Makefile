@@ -2,7 +2,7 @@
 #
 #   make            libgapbs_graph.so (host builder), libgapbs_pr.so (CUDA
 #                   engine, sm_100a), pr_gpu (the pr_spmv-compatible CLI),
-#                   cc_gpu (the cc-compatible CLI)
+#                   cc_gpu and bfs_gpu (the cc- and bfs-compatible CLIs)
 #   make oracle     oracle/liboracle.so and, where the reference tree exists,
 #                   oracle/_ref/ (test infrastructure only)
 #
@@ -33,7 +33,7 @@ all: graph engine cli
 
 graph: $(LIB)/libgapbs_graph.so
 engine: $(LIB)/libgapbs_pr.so
-cli: $(BIN)/pr_gpu $(BIN)/cc_gpu
+cli: $(BIN)/pr_gpu $(BIN)/cc_gpu $(BIN)/bfs_gpu
 
 $(LIB)/libgapbs_graph.so: $(HOST_SRCS) $(HOST_HDRS)
 	mkdir -p $(LIB)
@@ -55,6 +55,11 @@ $(BIN)/pr_gpu: $(SRC)/host/pr_main.cc $(HOST_SRCS) $(HOST_HDRS) $(LIB)/libgapbs_
 $(BIN)/cc_gpu: $(SRC)/host/cc_main.cc $(HOST_SRCS) $(HOST_HDRS) $(LIB)/libgapbs_pr.so include/pr_gpu.h
 	mkdir -p $(BIN)
 	$(CXX) $(HOST_CXXFLAGS) $(SRC)/host/cc_main.cc $(HOST_SRCS) -o $@ \
+	    -L$(LIB) -lgapbs_pr -Wl,-rpath,'$$ORIGIN/../lib'
+
+$(BIN)/bfs_gpu: $(SRC)/host/bfs_main.cc $(HOST_SRCS) $(HOST_HDRS) $(LIB)/libgapbs_pr.so include/pr_gpu.h
+	mkdir -p $(BIN)
+	$(CXX) $(HOST_CXXFLAGS) $(SRC)/host/bfs_main.cc $(HOST_SRCS) -o $@ \
 	    -L$(LIB) -lgapbs_pr -Wl,-rpath,'$$ORIGIN/../lib'
 
 oracle:

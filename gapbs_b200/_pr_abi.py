@@ -16,7 +16,8 @@ PR_GPU_ERANGE = -6
 # Every symbol include/pr_gpu.h declares.
 SYMBOLS = (
     "pr_gpu_create", "pr_gpu_upload", "pr_gpu_upload_sg", "pr_gpu_generate", "pr_gpu_download_csr",
-    "pr_gpu_run", "pr_gpu_run_device", "pr_gpu_connected_components",
+    "pr_gpu_run", "pr_gpu_run_device", "pr_gpu_bfs", "pr_gpu_bfs_device",
+    "pr_gpu_connected_components",
     "pr_gpu_connected_components_device",
     "pr_gpu_adjoint", "pr_gpu_adjoint_device", "pr_gpu_set_stream",
     "pr_gpu_set_batch_tile", "pr_gpu_get_batch_tile", "pr_gpu_last_timing",
@@ -29,6 +30,10 @@ def declare(lib):
     lib.pr_gpu_create.restype = c_int
     lib.pr_gpu_upload.argtypes = [P, c_int64, c_int64, P, P, P, P, P]
     lib.pr_gpu_upload.restype = c_int
+    lib.pr_gpu_bfs.argtypes = [P, c_int64, P, P, c_int, POINTER(c_int)]
+    lib.pr_gpu_bfs.restype = c_int
+    lib.pr_gpu_bfs_device.argtypes = [P, c_int64, P, P, c_int, POINTER(c_int)]
+    lib.pr_gpu_bfs_device.restype = c_int
     lib.pr_gpu_connected_components.argtypes = [P, P]
     lib.pr_gpu_connected_components.restype = c_int
     lib.pr_gpu_connected_components_device.argtypes = [P, P]

@@ -173,6 +173,26 @@ struct CcScratch {
   int64_t cap = 0;
 };
 void FreeCcScratch(CcScratch *c);
+
+// Breadth-first search (bfs.cu).  Work arrays kept between calls.
+struct BfsScratch {
+  int32_t *parent = nullptr, *queue[2] = {nullptr, nullptr};
+  unsigned *bm[2] = {nullptr, nullptr};
+  int64_t *deg = nullptr, *eoff = nullptr;
+  void *cnt = nullptr, *tmp = nullptr;
+  int64_t cap_n = 0, cap_tmp = 0;
+};
+struct BfsStep {
+  const char *kind;  // "i", "td", "e", "bu", "c" as the reference logs them
+  int64_t count;     // frontier size after td, awake count after bu, else -1
+  double seconds;
+};
+void FreeBfsScratch(BfsScratch *b);
+// parent_old[v] (device, n entries, original ids): v's BFS parent from
+// source_old, the source itself for the source, -1 when unreached.
+cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t s,
+                               int source_old, int alpha, int beta, int32_t *parent_old,
+                               std::vector<BfsStep> *steps, std::string *err);
 cudaError_t ConnectedComponents(const DeviceGraph &g, CcScratch &cs, cudaStream_t s,
                                 int32_t *out_old, std::string *err);
 // int64 CSR offsets -> int32, setting *bad for values outside [0, 2^31).

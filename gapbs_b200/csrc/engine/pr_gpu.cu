@@ -40,7 +40,8 @@ struct pr_gpu {
   // CSR of the last pr_gpu_generate (original ids), kept for download
   int32_t *gen_off = nullptr, *gen_nbr = nullptr;
   int64_t gen_n = 0, gen_m = 0;
-  prgpu::CcScratch cc;  // connected-components work arrays
+  prgpu::CcScratch cc;    // connected-components work arrays
+  prgpu::BfsScratch bfs;  // breadth-first-search work arrays
 };
 
 namespace {
@@ -444,6 +445,7 @@ void pr_gpu_destroy(pr_gpu_t *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   FreeGenerated(h);
   prgpu::FreeCcScratch(&h->cc);
+  prgpu::FreeBfsScratch(&h->bfs);
   h->loop_single.Reset();
   h->loop_adjoint.Reset();
   prgpu::FreeDeviceGraph(&h->g);
@@ -637,6 +639,46 @@ int pr_gpu_connected_components_device(pr_gpu_t *h, int32_t *comp_out_dev) {
   cudaError_t e = prgpu::ConnectedComponents(h->g, h->cc, h->stream, comp_out_dev, &msg);
   if (e != cudaSuccess) return SetErr(h, PR_GPU_ECUDA, msg);
   return PR_GPU_OK;
+}
+
+int pr_gpu_bfs_device(pr_gpu_t *h, int64_t source, int32_t *parent_out_dev,
+                      pr_gpu_bfs_step_t *steps, int max_steps, int *nsteps) {
+  if (!h) return PR_GPU_EINVAL;
+  if (!h->has_graph) return SetErr(h, PR_GPU_ENOGRAPH, "no graph uploaded");
+  if (!parent_out_dev) return SetErr(h, PR_GPU_EINVAL, "parent_out is null");
+  if (source < 0 || source >= h->g.n) return SetErr(h, PR_GPU_EINVAL, "source out of range");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  std::string msg;
+  std::vector<prgpu::BfsStep> log;
+  cudaError_t e = prgpu::BreadthFirstSearch(h->g, h->bfs, h->stream, static_cast<int>(source), 15,
+                                            18, parent_out_dev, &log, &msg);
+  if (e != cudaSuccess)
+    return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
+  int k = 0;
+  for (const prgpu::BfsStep &st : log) {
+    if (!steps || k >= max_steps) break;
+    std::memset(steps[k].kind, 0, sizeof(steps[k].kind));
+    std::strncpy(steps[k].kind, st.kind, sizeof(steps[k].kind) - 1);
+    steps[k].count = st.count;
+    steps[k].seconds = st.seconds;
+    k++;
+  }
+  if (nsteps) *nsteps = static_cast<int>(log.size());
+  return PR_GPU_OK;
+}
+
+int pr_gpu_bfs(pr_gpu_t *h, int64_t source, int32_t *parent_out, pr_gpu_bfs_step_t *steps,
+               int max_steps, int *nsteps) {
+  if (!h) return PR_GPU_EINVAL;
+  if (!h->has_graph) return SetErr(h, PR_GPU_ENOGRAPH, "no graph uploaded");
+  if (!parent_out) return SetErr(h, PR_GPU_EINVAL, "parent_out is null");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  int32_t *d = nullptr;
+  PR_CHECK(h, cudaMalloc(&d, sizeof(int32_t) * h->g.n));
+  int rc = pr_gpu_bfs_device(h, source, d, steps, max_steps, nsteps);
+  if (!rc) rc = CopyToHost(h, parent_out, d, sizeof(int32_t) * h->g.n);
+  cudaFree(d);
+  return rc;
 }
 
 int pr_gpu_connected_components(pr_gpu_t *h, int32_t *comp_out) {

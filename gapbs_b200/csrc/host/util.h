@@ -31,6 +31,17 @@ inline void PrintStep(int step, double value) {
   std::printf("%5s%23.5lf\n", std::to_string(step).c_str(), value);
 }
 
+// The labelled step lines of the reference's -l logging (src/util.h:33-42).
+inline void PrintStep(const std::string &s, int64_t count) {
+  std::printf("%-14s%14lld\n", (s + ":").c_str(), static_cast<long long>(count));
+}
+inline void PrintStep(const std::string &s, double seconds, int64_t count = -1) {
+  if (count != -1)
+    std::printf("%5s%11lld  %10.5lf\n", s.c_str(), static_cast<long long>(count), seconds);
+  else
+    std::printf("%5s%23.5lf\n", s.c_str(), seconds);
+}
+
 class WallTimer {
  public:
   void Start() { t0_ = t1_ = Clock::now(); }

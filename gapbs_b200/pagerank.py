@@ -110,6 +110,29 @@ class PageRankEngine:
         else:
             self.upload_csr(g.num_nodes, g.out_offsets, g.out_neighbors, None, None, edge_w)
 
+    def bfs(self, source: int, with_steps: bool = False):
+        """Direction-optimizing BFS from `source`: parent of every vertex
+        (the source for itself, -1 when unreachable).  with_steps: also the
+        step log [(kind, count, seconds)] as the reference prints it with -l."""
+        parent = np.empty(self.n, np.int32)
+        steps = np.zeros(256, dtype=np.dtype([("kind", "S4"), ("count", "<i8"), ("seconds", "<f8")],
+                                             align=True))  # pr_gpu_bfs_step_t, 24 bytes
+        nsteps = ctypes.c_int()
+        self._check(self._lib.pr_gpu_bfs(self._h, int(source), _ptr(parent), _ptr(steps),
+                                         steps.size, byref(nsteps)), "pr_gpu_bfs")
+        if not with_steps:
+            return parent
+        k = min(nsteps.value, steps.size)
+        return parent, [(s["kind"].decode(), int(s["count"]), float(s["seconds"]))
+                        for s in steps[:k]]
+
+    def bfs_device(self, source: int, parent_ptr: int) -> int:
+        """BFS parents into a device buffer of n int32; returns the step count."""
+        nsteps = ctypes.c_int()
+        self._check(self._lib.pr_gpu_bfs_device(self._h, int(source), parent_ptr, None, 0,
+                                                byref(nsteps)), "pr_gpu_bfs_device")
+        return nsteps.value
+
     def connected_components(self) -> np.ndarray:
         """Component label of every vertex of the uploaded graph: the smallest
         vertex id of its component (the reference's Afforest labelling)."""

@@ -99,6 +99,30 @@ int pr_gpu_generate(pr_gpu_t *h, int uniform, int scale, int degree,
  * offsets, m_out neighbours), then frees the device copy. */
 int pr_gpu_download_csr(pr_gpu_t *h, int64_t *out_off, int32_t *out_nbr);
 
+/* One step of a breadth-first search as the reference logs it with -l
+ * (src/bfs.cc:118-160): kind "i" (init), "td" (top-down; count = next
+ * frontier size), "e" (queue to bitmap), "bu" (bottom-up; count = vertices
+ * found), "c" (bitmap to queue); count -1 where the reference prints none. */
+typedef struct pr_gpu_bfs_step {
+  char kind[4];
+  int64_t count;
+  double seconds;
+} pr_gpu_bfs_step_t;
+
+/* Direction-optimizing breadth-first search from `source` (original id) over
+ * the uploaded graph, the reference's DOBFS (src/bfs.cc:38-174: the same
+ * top-down / bottom-up steps and switching rule, alpha 15, beta 18).
+ * parent_out[v] (n entries, original ids) = v's parent in a BFS tree, the
+ * source for the source, -1 when unreachable; depths along the tree are BFS
+ * depths, so the reference's BFSVerifier (src/bfs.cc:201-245) accepts
+ * it.  Which of several same-depth candidates becomes a parent is a race,
+ * as in the reference.  steps (nullable): the first max_steps steps;
+ * *nsteps: their total.  Host buffer / device buffer forms. */
+int pr_gpu_bfs(pr_gpu_t *h, int64_t source, int32_t *parent_out,
+               pr_gpu_bfs_step_t *steps, int max_steps, int *nsteps);
+int pr_gpu_bfs_device(pr_gpu_t *h, int64_t source, int32_t *parent_out_dev,
+                      pr_gpu_bfs_step_t *steps, int max_steps, int *nsteps);
+
 /* Connected components of the uploaded graph, the reference's Afforest
  * (src/cc.cc:40-150: two neighbour-sampling rounds, the largest
  * intermediate component skipped in the final link phase, a directed graph

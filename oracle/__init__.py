@@ -45,6 +45,10 @@ def lib() -> ctypes.CDLL:
         L.oracle_pr_verify_f32.restype = c_double
         L.oracle_pr_residual_f64.argtypes = [c_int64, P, P, P, c_float, P]
         L.oracle_pr_residual_f64.restype = c_double
+        L.oracle_bfs_depths.argtypes = [c_int64, P, P, c_int, P]
+        L.oracle_bfs_depths.restype = None
+        L.oracle_bfs_verify.argtypes = [c_int64, P, P, P, P, c_int, P]
+        L.oracle_bfs_verify.restype = c_int
         L.oracle_cc_afforest.argtypes = [c_int64, P, P, P, P, c_int, P]
         L.oracle_cc_afforest.restype = None
         L.oracle_ppr_residual_f64.argtypes = [c_int64, P, P, P, c_float, P, P]
@@ -112,6 +116,53 @@ def cc_afforest(g) -> np.ndarray:
     lib().oracle_cc_afforest(n, _ptr(oo), _ptr(on), _ptr(io), _ptr(inb), int(g.directed),
                              _ptr(comp))
     return comp
+
+
+def bfs_depths(g, source: int) -> np.ndarray:
+    """BFS depths from source (-1 unreachable), the reference verifier's search."""
+    oo = np.ascontiguousarray(g.out_offsets, np.int64)
+    on = np.ascontiguousarray(g.out_neighbors, np.int32)
+    depth = np.empty(g.num_nodes, np.int32)
+    lib().oracle_bfs_depths(g.num_nodes, _ptr(oo), _ptr(on), int(source), _ptr(depth))
+    return depth
+
+
+def bfs_verify(g, source: int, parent) -> bool:
+    """The reference's BFSVerifier restated."""
+    oo = np.ascontiguousarray(g.out_offsets, np.int64)
+    on = np.ascontiguousarray(g.out_neighbors, np.int32)
+    io = np.ascontiguousarray(g.in_offsets, np.int64)
+    inb = np.ascontiguousarray(g.in_neighbors, np.int32)
+    p = np.ascontiguousarray(parent, np.int32)
+    return bool(lib().oracle_bfs_verify(g.num_nodes, _ptr(oo), _ptr(on), _ptr(io), _ptr(inb),
+                                        int(source), _ptr(p)))
+
+
+def ref_bfs(args: str, k: int = 1, source: int = -1, run: bool = True):
+    """The reference's SourcePicker and DOBFS on the graph its builder makes
+    for args.  Returns (first k picked sources, parents from `source` or the
+    first pick, kernel seconds); parents is None when run is False."""
+    path = os.path.join(REF_DIR, "libgapbs_ref_bfs.so")
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} missing (built by `make -C oracle` where the reference "
+                           "tree exists)")
+    R = ctypes.CDLL(path)
+    R.ref_bfs.argtypes = [c_int, POINTER(c_char_p), c_int, P, c_int64, P, c_int64,
+                          POINTER(c_double)]
+    R.ref_bfs.restype = c_int64
+    toks = ["bfs"] + args.split()
+    argv = (c_char_p * len(toks))(*[t.encode() for t in toks])
+    srcs = np.empty(max(k, 1), np.int32)
+    sec = c_double()
+    n = R.ref_bfs(len(toks), argv, k, _ptr(srcs), -1, None, 0, ctypes.byref(sec))
+    if n < 0:
+        raise RuntimeError(f"reference rejected {args!r}")
+    parent = None
+    if run:
+        parent = np.empty(n, np.int32)
+        R.ref_bfs(len(toks), argv, k, _ptr(srcs), int(source), _ptr(parent), n,
+                  ctypes.byref(sec))
+    return srcs[:k], parent, float(sec.value)
 
 
 def ref_cc_afforest(args: str):

@@ -289,3 +289,54 @@ void oracle_cc_afforest(int64_t n, const int64_t *out_off, const int32_t *out_nb
   }
   cc_compress(n, comp);
 }
+
+/* ---- breadth-first search (src/bfs.cc) ---------------------------------- */
+
+void oracle_bfs_depths(int64_t n, const int64_t *out_off, const int32_t *out_nbr,
+                       int32_t source, int32_t *depth) {
+  int32_t *queue = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+  for (int64_t v = 0; v < n; v++) depth[v] = -1;
+  int64_t head = 0, tail = 0;
+  depth[source] = 0;
+  queue[tail++] = source;
+  while (head < tail) {
+    const int32_t u = queue[head++];
+    for (int64_t e = out_off[u]; e < out_off[u + 1]; e++) {
+      const int32_t v = out_nbr[e];
+      if (depth[v] == -1) {
+        depth[v] = depth[u] + 1;
+        queue[tail++] = v;
+      }
+    }
+  }
+  free(queue);
+}
+
+int oracle_bfs_verify(int64_t n, const int64_t *out_off, const int32_t *out_nbr,
+                      const int64_t *in_off, const int32_t *in_nbr, int32_t source,
+                      const int32_t *parent) {
+  int32_t *depth = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+  oracle_bfs_depths(n, out_off, out_nbr, source, depth);
+  int ok = 1;
+  for (int64_t u = 0; u < n && ok; u++) {
+    if (depth[u] != -1 && parent[u] != -1) {
+      if (u == source) {
+        if (!(parent[u] == u && depth[u] == 0)) ok = 0;
+        continue;
+      }
+      int found = 0;
+      for (int64_t e = in_off[u]; e < in_off[u + 1]; e++) {
+        if (in_nbr[e] == parent[u]) {
+          if (depth[in_nbr[e]] != depth[u] - 1) ok = 0;
+          found = 1;
+          break;
+        }
+      }
+      if (!found) ok = 0;
+    } else if (depth[u] != parent[u]) {
+      ok = 0;
+    }
+  }
+  free(depth);
+  return ok;
+}

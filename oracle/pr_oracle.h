@@ -107,6 +107,19 @@ void oracle_cc_afforest(int64_t n, const int64_t *out_off, const int32_t *out_nb
                         const int64_t *in_off, const int32_t *in_nbr, int directed,
                         int32_t *comp);
 
+/* Breadth-first depths from source (-1 when unreachable), the serial search
+ * of the reference's BFSVerifier (src/bfs.cc:203-215). */
+void oracle_bfs_depths(int64_t n, const int64_t *out_off, const int32_t *out_nbr,
+                       int32_t source, int32_t *depth);
+
+/* The reference's BFSVerifier (src/bfs.cc:201-245): 1 when parent[] is a
+ * BFS tree from source (the source its own parent at depth 0, every other
+ * reached vertex's parent an in-neighbour one level up, unreached vertices
+ * -1), else 0. */
+int oracle_bfs_verify(int64_t n, const int64_t *out_off, const int32_t *out_nbr,
+                      const int64_t *in_off, const int32_t *in_nbr, int32_t source,
+                      const int32_t *parent);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,7 +34,14 @@ from its own sources by oracle/Makefile) exist.  Writes:
                                      labels, the labels themselves for the
                                      smallest graphs
 
-Usage:  python tests/golden/make_golden.py [--fullsize | --cli | --cc]
+  bfs_golden.json                    (--bfs) the reference's SourcePicker
+                                     sources and, per source, what its DOBFS
+                                     tree gives: reached count, PrintBFSStats
+                                     edge count, sha256 of the depths along
+                                     its parent pointers (the depths themselves
+                                     for the smallest graphs)
+
+Usage:  python tests/golden/make_golden.py [--fullsize | --cli | --cc | --bfs]
 """
 from __future__ import annotations
 
@@ -252,6 +259,9 @@ CLI_CASES = ["-h", "-f {tmp}/missing.el", "-f {tmp}/x.foo", "-g", "-z", "-n"]
 
 # cc -a runs whose analysis lines (clusters, component count) are recorded
 CC_ANALYSIS_CASES = ["-g 10 -n 1 -a", "-u 12 -k 1 -n 1 -a", "-f {graphs}/4.el -n 1 -a"]
+# bfs -a runs whose "BFS Tree has ..." line (last trial's source) is recorded
+BFS_ANALYSIS_CASES = ["-g 10 -n 3 -a", "-u 12 -k 1 -n 2 -a", "-f {graphs}/4.el -n 3 -a",
+                      "-g 12 -r 5 -n 1 -a", "-f {graphs}/4.el -s -n 2 -a"]
 
 
 def main_cli():
@@ -259,7 +269,7 @@ def main_cli():
     out = {"generator": "tests/golden/make_golden.py --cli", "cases": [], "cc_analysis": []}
     with tempfile.TemporaryDirectory() as tmp:
         open(os.path.join(tmp, "x.foo"), "w").close()
-        for binary in ("pr_spmv", "cc"):
+        for binary in ("pr_spmv", "cc", "bfs"):
             exe = os.path.join(ROOT, "oracle", "_ref", binary)
             if not os.path.exists(exe):
                 sys.exit(f"needs oracle/_ref/{binary} (make -C oracle where the reference tree exists)")
@@ -278,6 +288,13 @@ def main_cli():
         j = next(k for k, ln in enumerate(lines) if ln.startswith("There are "))
         out["cc_analysis"].append({"args": args, "lines": lines[i - 1:j + 1]})
         print("cc", args, lines[j])
+    out["bfs_analysis"] = []
+    exe = os.path.join(ROOT, "oracle", "_ref", "bfs")
+    for args in BFS_ANALYSIS_CASES:
+        p = subprocess.run([exe] + args.format(graphs=gdir).split(), capture_output=True, text=True)
+        line = next(ln for ln in p.stdout.splitlines() if ln.startswith("BFS Tree has "))
+        out["bfs_analysis"].append({"args": args, "line": line})
+        print("bfs", args, line)
     with open(os.path.join(HERE, "cli_golden.json"), "w") as fh:
         json.dump(out, fh, indent=1)
 
@@ -308,8 +325,60 @@ def main_cc():
         json.dump(out, fh, separators=(",", ":"))
 
 
+BFS_CASES = [
+    ("g10", "-g 10", True), ("u10", "-u 10", True), ("g12k4", "-g 12 -k 4", True),
+    ("u12k1", "-u 12 -k 1", True), ("g14", "-g 14", False), ("g16", "-g 16", False),
+    ("el4", "-f {graphs}/4.el", True), ("el4s", "-f {graphs}/4.el -s", True),
+    ("mtx4", "-f {graphs}/4.mtx", True),
+]
+
+
+def depths_from_parents(parent, src):
+    """Depth of every vertex along the parent pointers (-1 unreached)."""
+    n = parent.size
+    d = np.full(n, -1, np.int32)
+    d[src] = 0
+    level = np.array([src])
+    k = 0
+    not_src = np.arange(n) != src
+    while level.size:
+        nxt = np.nonzero(np.isin(parent, level) & (d == -1) & not_src)[0]
+        k += 1
+        d[nxt] = k
+        level = nxt
+    return d
+
+
+def main_bfs():
+    from gapbs_b200.graph import make_graph
+    gdir = os.path.join(HERE, "graphs")
+    out = {"generator": "tests/golden/make_golden.py --bfs", "cases": {}}
+    for name, args, keep in BFS_CASES:
+        a = args.format(graphs=gdir)
+        (srcs, _, _), _ = capture_stdout(oracle.ref_bfs, a, 3, -1, False)
+        g = make_graph(a)
+        odeg = np.diff(g.out_offsets)
+        runs = []
+        for src in srcs:
+            (_, parent, _), _ = capture_stdout(oracle.ref_bfs, a, 3, int(src), True)
+            d = depths_from_parents(parent, int(src))
+            reached = parent >= 0
+            run = {"source": int(src), "reached": int(reached.sum()),
+                   "tree_edges": int(odeg[reached].sum()), "depth_sha256": sha(d),
+                   "max_depth": int(d.max())}
+            if keep:
+                run["depths"] = [int(x) for x in d]
+            runs.append(run)
+        out["cases"][name] = {"args": args, "num_nodes": g.num_nodes, "runs": runs}
+        print(name, [r["source"] for r in runs], [r["reached"] for r in runs])
+    with open(os.path.join(HERE, "bfs_golden.json"), "w") as fh:
+        json.dump(out, fh, separators=(",", ":"))
+
+
 if __name__ == "__main__":
-    if "--fullsize" in sys.argv[1:]:
+    if "--bfs" in sys.argv[1:]:
+        main_bfs()
+    elif "--fullsize" in sys.argv[1:]:
         main_fullsize()
     elif "--cli" in sys.argv[1:]:
         main_cli()
@@ -319,3 +388,4 @@ if __name__ == "__main__":
         main()
         main_cli()
         main_cc()
+        main_bfs()

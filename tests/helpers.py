@@ -32,3 +32,19 @@ def row_sums(g, ew):
     src = np.repeat(np.arange(g.num_nodes), np.diff(g.out_offsets))
     np.add.at(out, src, ew.astype(np.float64))
     return out
+
+
+def depths_from_parents(parent, src):
+    """Depth of every vertex along BFS parent pointers (-1 unreached)."""
+    n = parent.size
+    d = np.full(n, -1, np.int32)
+    d[src] = 0
+    level = np.array([src])
+    k = 0
+    not_src = np.arange(n) != src
+    while level.size:
+        nxt = np.nonzero(np.isin(parent, level) & (d == -1) & not_src)[0]
+        k += 1
+        d[nxt] = k
+        level = nxt
+    return d

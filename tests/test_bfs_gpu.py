@@ -1,0 +1,96 @@
+"""Direction-optimizing BFS on the GPU (pr_gpu_bfs) against the reference.
+
+Parents may differ from the reference's (which same-depth candidate claims a
+vertex is a race there too), so the checks are the reference's own verifier
+(restated in the oracle) and what any BFS tree from the source determines:
+the depths along the parent pointers, the reached set and the tree's edge
+count, against the reference's DOBFS results in tests/golden/bfs_golden.json
+and the oracle's search.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from gapbs_b200 import PageRankEngine
+from gapbs_b200.graph import Graph, make_graph
+from gapbs_b200.pagerank import PageRankError
+from conftest import GOLDEN, gpu_available
+from helpers import depths_from_parents
+
+pytestmark = pytest.mark.gpu
+
+with open(os.path.join(GOLDEN, "bfs_golden.json")) as fh:
+    CASES = json.load(fh)["cases"]
+
+
+@pytest.fixture(scope="module")
+def engine():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    eng = PageRankEngine(0)
+    yield eng
+    eng.close()
+
+
+def check(g, src, parent):
+    assert oracle.bfs_verify(g, src, parent)
+    assert np.array_equal(depths_from_parents(parent, src), oracle.bfs_depths(g, src))
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_gpu_matches_reference(engine, name):
+    e = CASES[name]
+    g = make_graph(e["args"].format(graphs=os.path.join(GOLDEN, "graphs")))
+    engine.upload(g)
+    odeg = np.diff(g.out_offsets)
+    for run in e["runs"]:
+        parent = engine.bfs(run["source"])
+        assert oracle.bfs_verify(g, run["source"], parent)
+        d = depths_from_parents(parent, run["source"])
+        assert hashlib.sha256(d.tobytes()).hexdigest() == run["depth_sha256"]
+        assert int((parent >= 0).sum()) == run["reached"]
+        assert int(odeg[parent >= 0].sum()) == run["tree_edges"]
+
+
+@pytest.mark.parametrize("args", ["-g 20", "-u 20", "-g 18 -k 2", "-u 16 -k 1"])
+def test_gpu_bfs_larger_graphs(engine, args):
+    g = make_graph(args)
+    engine.upload(g)
+    rng = np.random.default_rng(1)
+    cand = np.nonzero(np.diff(g.out_offsets) > 0)[0]
+    for src in rng.choice(cand, 3, replace=False):
+        parent, steps = engine.bfs(int(src), with_steps=True)
+        check(g, int(src), parent)
+        assert steps[0][0] == "i"
+        assert {k for k, _, _ in steps} <= {"i", "td", "e", "bu", "c"}
+
+
+def test_directed_and_adversarial(engine):
+    rng = np.random.default_rng(6)
+    d = Graph.from_edges(rng.integers(0, 20000, 80000), rng.integers(0, 20000, 80000))
+    engine.upload(d)
+    for src in (0, 17, 4242):
+        check(d, src, engine.bfs(src))
+    adv = np.load(os.path.join(GOLDEN, "adversarial.npz"))
+    for name in ("isolated", "star", "chain", "directed_sinks", "selfdup", "hub5000"):
+        g = Graph.from_edges(adv[f"{name}_u"], adv[f"{name}_v"], symmetrize=bool(adv[f"{name}_sym"]))
+        engine.upload(g)
+        for src in {0, g.num_nodes - 1, g.num_nodes // 2}:
+            check(g, src, engine.bfs(src))
+
+
+def test_generated_graph_and_errors(engine):
+    engine.generate("-g 16")
+    e = CASES["g16"]
+    src = e["runs"][0]["source"]
+    parent = engine.bfs(src)
+    d = depths_from_parents(parent, src)
+    assert hashlib.sha256(d.tobytes()).hexdigest() == e["runs"][0]["depth_sha256"]
+    with pytest.raises(PageRankError):
+        engine.bfs(-1)
+    with pytest.raises(PageRankError):
+        engine.bfs(engine.n)

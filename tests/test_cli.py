@@ -1,5 +1,5 @@
-"""The pr_gpu / cc_gpu command lines against the reference's pr_spmv / cc
-(no GPU needed).
+"""The pr_gpu / cc_gpu / bfs_gpu command lines against the reference's
+pr_spmv / cc / bfs (no GPU needed).
 
 Help text, and every invocation that the reference rejects before running a
 kernel, must give the reference's exit code and stdout byte for byte
@@ -14,7 +14,7 @@ import pytest
 from conftest import GOLDEN, ROOT
 
 BIN = os.path.join(ROOT, "gapbs_b200", "bin")
-OURS = {"pr_spmv": "pr_gpu", "cc": "cc_gpu"}  # reference binary -> drop-in
+OURS = {"pr_spmv": "pr_gpu", "cc": "cc_gpu", "bfs": "bfs_gpu"}  # reference binary -> drop-in
 with open(os.path.join(GOLDEN, "cli_golden.json")) as fh:
     CASES = json.load(fh)["cases"]
 

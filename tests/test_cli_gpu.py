@@ -14,8 +14,11 @@ from conftest import GOLDEN, ROOT, gpu_available
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(ROOT, "gapbs_b200", "bin", "pr_gpu")
 CC_EXE = os.path.join(ROOT, "gapbs_b200", "bin", "cc_gpu")
+BFS_EXE = os.path.join(ROOT, "gapbs_b200", "bin", "bfs_gpu")
 with open(os.path.join(GOLDEN, "cli_golden.json")) as fh:
-    CC_ANALYSIS = json.load(fh)["cc_analysis"]
+    _CLI = json.load(fh)
+CC_ANALYSIS = _CLI["cc_analysis"]
+BFS_ANALYSIS = _CLI["bfs_analysis"]
 with open(os.path.join(GOLDEN, "pr_golden.json")) as fh:
     GOLD = json.load(fh)["cases"]
 STEP = re.compile(r"^ {4}\d+ +\d+\.\d{5}$")
@@ -74,3 +77,20 @@ def test_cc_verification_on_larger_graphs(exe):
     for args in ("-g 16 -n 2 -v", "-u 16 -k 2 -n 1 -v"):
         out = run(CC_EXE, args.split())
         assert out.count("Verification:           PASS") == int(args.split()[args.split().index("-n") + 1])
+
+
+@pytest.mark.parametrize("case", BFS_ANALYSIS, ids=[c["args"] for c in BFS_ANALYSIS])
+def test_bfs_analysis_and_verification(exe, case):
+    args = case["args"].format(graphs=os.path.join(GOLDEN, "graphs")).split() + ["-v"]
+    out = run(BFS_EXE, args)
+    assert case["line"] in out.splitlines()
+    trials = int(args[args.index("-n") + 1])
+    assert out.count("Verification:           PASS") == trials
+
+
+def test_bfs_logging_lines(exe):
+    out = run(BFS_EXE, ["-g", "14", "-n", "1", "-l"])
+    lines = out.splitlines()
+    assert any(ln.startswith("Source:") for ln in lines)
+    kinds = [ln.split()[0] for ln in lines if ln.split() and ln.split()[0] in ("i", "td", "e", "bu", "c")]
+    assert kinds and kinds[0] == "i"
