@@ -58,6 +58,8 @@ def parse_args():
     p.add_argument("--adjoint-graph", default="-g 20")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-cc", action="store_true")
+    p.add_argument("--no-bfs", action="store_true")
+    p.add_argument("--bfs-sources", type=int, default=8)
     p.add_argument("--e2e-upload-steps", type=int, default=3,
                    help="steps of the end-to-end variant that uploads the graph every step")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -357,6 +359,39 @@ def run_ours(a, dist: Dist):
               "components": int(torch.unique(comp).numel())}
         eng.set_stream(None)
 
+    # ---- direction-optimizing BFS from fixed sources on the same graph
+    bfs = None
+    if not a.no_bfs:
+        parent = torch.empty(n, dtype=torch.int32, device=f"cuda:{dev}")
+        rng = np.random.default_rng(27491095 + 4)
+        bfs_sources = [int(x) for x in rng.integers(0, n, 4 * a.bfs_sources)]
+        eng.set_stream(stream.cuda_stream)
+        for s_ in bfs_sources[:2]:
+            eng.bfs_device(s_, parent.data_ptr())  # warm-up (also checks the sources)
+        torch.cuda.synchronize()
+        picked, t_total, steps_total = [], 0.0, 0
+        for s_ in bfs_sources:
+            if len(picked) == a.bfs_sources:
+                break
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            nst = eng.bfs_device(s_, parent.data_ptr())
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            if nst <= 2:
+                continue  # an isolated source: nothing to search
+            picked.append(s_)
+            t_total += dt
+            steps_total += nst
+        bfs_ms = dist.max(t_total * 1e3 / max(1, len(picked)))
+        bfs = {"workload": f"direction-optimizing BFS of {a.graph.strip()} from {len(picked)} "
+                           "sources with out-edges (seeded draw)",
+               "ms": round(bfs_ms, 3), "unit": "ms per search (device-resident graph, host-"
+                                               "driven steps)",
+               "gteps": round(m / (bfs_ms / 1e3) / 1e9, 2), "steps_per_search":
+                   round(steps_total / max(1, len(picked)), 1), "sources": picked}
+        eng.set_stream(None)
+
     # ---- end to end with the graph uploaded every step (a caller whose graph
     # changes between solves): pr_gpu_upload of the host CSR + pr_gpu_run
     e2e_up = None
@@ -454,6 +489,8 @@ def run_ours(a, dist: Dist):
         result["e2e_graph_upload_each_step"] = e2e_up
     if cc is not None:
         result["cc"] = cc
+    if bfs is not None:
+        result["bfs"] = bfs
     del flush
 
     # ---- batched PPR vs sequential single-vector solves (rank 0, N=1 config)
@@ -467,6 +504,13 @@ def run_ours(a, dist: Dist):
         if g is None:
             g = eng.download_graph()  # the generated graph, for the reference on the host
         result["cpu_baseline"] = cpu_baseline(g, a, sweeps_per_step)
+        if bfs is not None and bfs["sources"]:
+            import oracle
+            if oracle.ref_available():
+                _, sec = oracle.ref_bfs_csr(g, bfs["sources"])
+                bfs["reference_cpu_ms"] = round(sec * 1e3 / len(bfs["sources"]), 3)
+                bfs["reference_cpu_cores"] = os.cpu_count() or 1
+                bfs["speedup_vs_reference_cpu"] = round(bfs["reference_cpu_ms"] / bfs["ms"], 2)
         if cc is not None:
             import oracle
             if oracle.ref_available():

@@ -165,6 +165,27 @@ def ref_bfs(args: str, k: int = 1, source: int = -1, run: bool = True):
     return srcs[:k], parent, float(sec.value)
 
 
+def ref_bfs_csr(g, sources):
+    """The reference's DOBFS on graph g's CSR from each source in turn.
+    Returns (last search's parents, total kernel seconds)."""
+    path = os.path.join(REF_DIR, "libgapbs_ref_bfs.so")
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} missing (built by `make -C oracle` where the reference "
+                           "tree exists)")
+    R = ctypes.CDLL(path)
+    R.ref_bfs_csr.argtypes = [c_int64, c_int, P, P, P, P, c_int, P, P]
+    R.ref_bfs_csr.restype = c_double
+    oo = np.ascontiguousarray(g.out_offsets, np.int64)
+    on = np.ascontiguousarray(g.out_neighbors, np.int32)
+    io = np.ascontiguousarray(g.in_offsets, np.int64)
+    inb = np.ascontiguousarray(g.in_neighbors, np.int32)
+    src = np.ascontiguousarray(sources, np.int32)
+    parent = np.empty(g.num_nodes, np.int32)
+    sec = R.ref_bfs_csr(g.num_nodes, int(g.directed), _ptr(oo), _ptr(on), _ptr(io), _ptr(inb),
+                        int(src.size), _ptr(src), _ptr(parent))
+    return parent, float(sec)
+
+
 def ref_cc_afforest(args: str):
     """The reference's own Afforest on the graph its builder makes for args
     (pr_spmv-style options).  Returns (labels, kernel seconds)."""

@@ -41,3 +41,48 @@ int64_t ref_bfs(int argc, char **argv, int k, int32_t *sources, int64_t source,
 }
 
 }  // extern "C"
+
+namespace {
+
+void CopyOffsetsBfs(pvector<SGOffset> *dst, int64_t n, const int64_t *off) {
+  for (int64_t i = 0; i <= n; i++) (*dst)[i] = off[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+// The reference's DOBFS on a CSR given by the caller, from each of the
+// nsrc sources in turn; returns the total kernel time in seconds and copies
+// the last search's parents into parent_out.
+double ref_bfs_csr(int64_t n, int directed, const int64_t *out_off, const int32_t *out_nbr,
+                   const int64_t *in_off, const int32_t *in_nbr, int nsrc,
+                   const int32_t *sources, int32_t *parent_out) {
+  pvector<SGOffset> offs(n + 1);
+  CopyOffsetsBfs(&offs, n, out_off);
+  NodeID *oneigh = new NodeID[out_off[n] > 0 ? out_off[n] : 1];
+  if (out_off[n]) std::memcpy(oneigh, out_nbr, sizeof(NodeID) * out_off[n]);
+  NodeID **oindex = Graph::GenIndex(offs, oneigh);
+  Graph g;
+  if (!directed) {
+    g = Graph(n, oindex, oneigh);
+  } else {
+    pvector<SGOffset> ioffs(n + 1);
+    CopyOffsetsBfs(&ioffs, n, in_off);
+    NodeID *ineigh = new NodeID[in_off[n] > 0 ? in_off[n] : 1];
+    if (in_off[n]) std::memcpy(ineigh, in_nbr, sizeof(NodeID) * in_off[n]);
+    NodeID **iindex = Graph::GenIndex(ioffs, ineigh);
+    g = Graph(n, oindex, oneigh, iindex, ineigh);
+  }
+  double total = 0;
+  for (int i = 0; i < nsrc; i++) {
+    auto t0 = std::chrono::steady_clock::now();
+    pvector<NodeID> parent = DOBFS(g, sources[i]);
+    auto t1 = std::chrono::steady_clock::now();
+    total += std::chrono::duration<double>(t1 - t0).count();
+    if (i == nsrc - 1 && parent_out) std::memcpy(parent_out, parent.data(), sizeof(int32_t) * n);
+  }
+  return total;
+}
+
+}  // extern "C"
