@@ -140,3 +140,21 @@ def test_adjoint_fullsize(engine):
 
     assert rel_l2(gt, gt64) <= 1e-4
     assert rel_l2(ge, gw64) <= 1e-3
+
+
+def test_cc_and_bfs_fullsize(engine):
+    """Connected components and BFS on the -g 25 graph: CC labels equal the
+    reference's Afforest on the same CSR; a BFS tree passes the reference's
+    verifier and its depths are the oracle's."""
+    from helpers import depths_from_parents
+    e = FULL["g25"]
+    engine.generate(e["args"])
+    g = engine.download_graph()
+    assert csr_sha(g) == e["csr_sha256"]
+    comp = engine.connected_components()
+    ref_comp, _ = oracle.ref_cc_afforest_csr(g, trials=1)
+    assert np.array_equal(comp, ref_comp)
+    src = int(np.nonzero(np.diff(g.out_offsets) > 0)[0][12345])
+    parent = engine.bfs(src)
+    assert oracle.bfs_verify(g, src, parent)
+    assert np.array_equal(depths_from_parents(parent, src), oracle.bfs_depths(g, src))
