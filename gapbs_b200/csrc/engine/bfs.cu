@@ -86,10 +86,11 @@ __global__ void bfs_frontier_degree_kernel(int64_t q, const int32_t *__restrict_
 
 // Top-down step over the frontier's edges: edge e belongs to the frontier
 // vertex i with eoff[i] <= e < eoff[i + 1] (eoff: exclusive scan of degrees).
-__global__ void bfs_td_kernel(int64_t q, int64_t edges, const int32_t *__restrict__ queue,
+__global__ void bfs_td_kernel(int64_t q, const int32_t *__restrict__ queue,
                               const int64_t *__restrict__ eoff, const int32_t *__restrict__ ooff,
                               const int32_t *__restrict__ onbr, int32_t *parent, int32_t *next,
                               BfsCounters *cnt) {
+  const int64_t edges = eoff[q];  // the scan's total: no host round trip
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   unsigned long long scout = 0;
   const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -172,13 +173,15 @@ __global__ void bfs_bitmap_to_queue_kernel(int32_t n, const unsigned *__restrict
   }
 }
 
-// parent < -1 -> -1, then original ids.
+// parent < -1 -> -1, in original ids: each original id gathers its row's
+// parent (coalesced writes; a scatter through perm wrote partial sectors).
 __global__ void bfs_finish_kernel(int32_t n, const int32_t *__restrict__ parent,
-                                  const int32_t *__restrict__ perm, int32_t *out_old) {
+                                  const int32_t *__restrict__ perm,
+                                  const int32_t *__restrict__ inv, int32_t *out_old) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride) {
-    const int32_t p = parent[v];
-    out_old[perm[v]] = p >= 0 ? perm[p] : -1;
+    const int32_t p = parent[inv[v]];
+    out_old[v] = p >= 0 ? perm[p] : -1;
   }
 }
 
@@ -323,15 +326,11 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
       size_t bytes = static_cast<size_t>(b.cap_tmp);
       BFS_TRY(cub::DeviceScan::ExclusiveSum(b.tmp, bytes, b.deg, b.eoff, static_cast<int>(qsize + 1),
                                             s));
-      int64_t edges = 0;
-      BFS_TRY(cudaMemcpyAsync(&edges, b.eoff + qsize, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
       BFS_TRY(cudaMemsetAsync(b.cnt, 0, sizeof(BfsCounters), s));
-      BFS_TRY(cudaStreamSynchronize(s));
-      if (edges > 0) {
-        bfs_td_kernel<<<BfsGrid(edges), 256, 0, s>>>(qsize, edges, b.queue[cur], b.eoff, ooff, onbr,
-                                                     b.parent, b.queue[cur ^ 1], cnt);
-        BFS_TRY(cudaGetLastError());
-      }
+      // grid sized by the largest edge count the frontier can have
+      bfs_td_kernel<<<BfsGrid(std::min<int64_t>(g.m, qsize * g.max_degree)), 256, 0, s>>>(
+          qsize, b.queue[cur], b.eoff, ooff, onbr, b.parent, b.queue[cur ^ 1], cnt);
+      BFS_TRY(cudaGetLastError());
       BFS_TRY(read_counters());
       scout_count = static_cast<int64_t>(hc.scout);
       qsize = static_cast<int64_t>(hc.qtail);
@@ -339,7 +338,8 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
       record("td", qsize, seconds(ts, clock::now()));
     }
   }
-  bfs_finish_kernel<<<grid, 256, 0, s>>>(static_cast<int32_t>(n), b.parent, g.perm, out_old);
+  bfs_finish_kernel<<<grid, 256, 0, s>>>(static_cast<int32_t>(n), b.parent, g.perm, g.inv,
+                                         out_old);
   BFS_TRY(cudaGetLastError());
   BFS_TRY(cudaStreamSynchronize(s));
   return cudaSuccess;

@@ -95,24 +95,42 @@ __global__ void cc_compress_kernel(int32_t n, int *comp, int *err) {
   }
 }
 
-// Final phase, one warp per vertex: out-neighbours from index `skip` on and,
-// for a directed graph, all in-neighbours; vertices of component `giant` are
-// skipped (src/cc.cc:122-146).
-__global__ void cc_finish_kernel(int32_t n, const int32_t *__restrict__ ooff,
-                                 const int32_t *__restrict__ onbr,
-                                 const int32_t *__restrict__ ioff,
-                                 const int32_t *__restrict__ inbr, int skip, int giant,
-                                 int *comp, int *err) {
+// Final phase: out-neighbours from index `skip` on and, for a directed graph,
+// all in-neighbours; vertices of component `giant` are skipped
+// (src/cc.cc:122-146).  Rows [row0, row1), one warp per vertex (the long
+// rows at the front of the degree-sorted mirror).
+__global__ void cc_finish_warp_kernel(int32_t row0, int32_t row1, const int32_t *__restrict__ ooff,
+                                      const int32_t *__restrict__ onbr,
+                                      const int32_t *__restrict__ ioff,
+                                      const int32_t *__restrict__ inbr, int skip, int giant,
+                                      int *comp, int *err) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t u = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; u < n;
-       u += warps) {
+  for (int64_t u = row0 + ((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+       u < row1; u += warps) {
     if (ld_comp(comp, static_cast<int>(u)) == giant) continue;
     for (int j = ooff[u] + skip + lane; j < ooff[u + 1]; j += 32)
       cc_link(static_cast<int>(u), onbr[j], comp, err);
     if (ioff)
       for (int j = ioff[u] + lane; j < ioff[u + 1]; j += 32)
         cc_link(static_cast<int>(u), inbr[j], comp, err);
+  }
+}
+
+// The same for rows [row0, row1), one thread per vertex (the short rows).
+__global__ void cc_finish_thread_kernel(int32_t row0, int32_t row1,
+                                        const int32_t *__restrict__ ooff,
+                                        const int32_t *__restrict__ onbr,
+                                        const int32_t *__restrict__ ioff,
+                                        const int32_t *__restrict__ inbr, int skip, int giant,
+                                        int *comp, int *err) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t u = row0 + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u < row1;
+       u += stride) {
+    if (ld_comp(comp, static_cast<int>(u)) == giant) continue;
+    for (int j = ooff[u] + skip; j < ooff[u + 1]; j++) cc_link(static_cast<int>(u), onbr[j], comp, err);
+    if (ioff)
+      for (int j = ioff[u]; j < ioff[u + 1]; j++) cc_link(static_cast<int>(u), inbr[j], comp, err);
   }
 }
 
@@ -195,21 +213,31 @@ cudaError_t ConnectedComponents(const DeviceGraph &g, CcScratch &cs, cudaStream_
   e = cudaMemsetAsync(derr, 0, sizeof(int), s);
   const unsigned grid = CcGrid(n);
   const int kRounds = 2;  // neighbor_rounds of src/cc.cc:92
+  // Rows without in-neighbours form the tail of the mirror; in an undirected
+  // graph they have no edges at all, so no link ever touches them and they
+  // stay their own components: the link and compress passes stop before them.
+  const int32_t active = g.directed ? n : static_cast<int32_t>(g.bin_row_start[kBinZero]);
+  // rows of at least 32 entries (the front of the mirror) take a warp each
+  const int32_t long_rows = std::min<int32_t>(active, static_cast<int32_t>(g.bin_row_start[4]));
   if (e == cudaSuccess) {
     cc_init_kernel<<<grid, 256, 0, s>>>(n, comp);
     for (int r = 0; r < kRounds; r++) {
-      cc_sample_kernel<<<grid, 256, 0, s>>>(n, ooff, onbr, r, comp, derr);
-      cc_compress_kernel<<<grid, 256, 0, s>>>(n, comp, derr);
+      cc_sample_kernel<<<grid, 256, 0, s>>>(active, ooff, onbr, r, comp, derr);
+      cc_compress_kernel<<<grid, 256, 0, s>>>(active, comp, derr);
     }
     e = cudaGetLastError();
   }
   const int giant = 0;  // the root, and label, of row 0's component
   if (e == cudaSuccess) {
-    const unsigned wgrid = CcGrid(static_cast<int64_t>(n) * 32);
-    cc_finish_kernel<<<wgrid, 256, 0, s>>>(n, ooff, onbr, g.directed ? g.rowoff : nullptr,
-                                           g.directed ? g.col : nullptr, kRounds, giant, comp,
-                                           derr);
-    cc_compress_kernel<<<grid, 256, 0, s>>>(n, comp, derr);
+    const int32_t *ioff = g.directed ? g.rowoff : nullptr;
+    const int32_t *inbr = g.directed ? g.col : nullptr;
+    if (long_rows > 0)
+      cc_finish_warp_kernel<<<CcGrid(static_cast<int64_t>(long_rows) * 32), 256, 0, s>>>(
+          0, long_rows, ooff, onbr, ioff, inbr, kRounds, giant, comp, derr);
+    if (active > long_rows)
+      cc_finish_thread_kernel<<<CcGrid(active - long_rows), 256, 0, s>>>(
+          long_rows, active, ooff, onbr, ioff, inbr, kRounds, giant, comp, derr);
+    cc_compress_kernel<<<grid, 256, 0, s>>>(active, comp, derr);
     fill_kernel<<<grid, 256, 0, s>>>(n, INT_MAX, root_min);
     cc_root_min_kernel<<<grid, 256, 0, s>>>(n, comp, g.perm, root_min);
     cc_label_kernel<<<grid, 256, 0, s>>>(n, comp, g.perm, root_min, out_old);
