@@ -2,13 +2,14 @@
 // mirror (pr_gpu_bfs in include/pr_gpu.h).
 //
 // The reference's DOBFS (src/bfs.cc:38-174), step for step:
-//   * parent[v] starts at -out_degree(v) (-1 without out-edges), the source
-//     is its own parent;
+//   * the source is its own parent;
 //   * top-down step: every frontier vertex claims its unvisited
 //     out-neighbours by compare-and-swap on parent[], the claimed vertices
 //     form the next frontier queue, and the step returns the scout count
-//     (the summed out-degrees of the claimed vertices, read back from the
-//     negative parents);
+//     (the summed out-degrees of the claimed vertices, 1 for a vertex
+//     without out-edges: the reference starts parent[v] at -out_degree(v),
+//     or -1, and adds the negated parent it replaced; here unvisited parents
+//     are all -1, set by one memset, and the degree is read at the claim);
 //   * bottom-up step: every unvisited vertex takes the first in-neighbour
 //     found in the frontier bitmap as its parent, the found vertices form the
 //     next bitmap, and the step returns their number;
@@ -52,28 +53,52 @@ __device__ __forceinline__ int32_t out_degree(const int32_t *ooff, int v) {
   return ooff[v + 1] - ooff[v];
 }
 
-// Warp-aggregated append of the flagged lanes' values to queue[] (tail).
-__device__ __forceinline__ void warp_append(bool flag, int value, int32_t *queue,
-                                            unsigned long long *tail) {
-  const unsigned mask = __activemask();
-  const unsigned ballot = __ballot_sync(mask, flag);
-  if (!ballot) return;
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(ballot) - 1;
-  unsigned long long base = 0;
-  if (lane == leader) base = atomicAdd(tail, static_cast<unsigned long long>(__popc(ballot)));
-  base = __shfl_sync(mask, base, leader);
-  if (flag) queue[base + __popc(ballot & ((1u << lane) - 1u))] = value;
+// The source (original id) becomes its own parent and the first frontier;
+// its out-degree is the first scout count.  One thread.
+__global__ void bfs_source_kernel(const int32_t *__restrict__ inv, int source_old,
+                                  const int32_t *__restrict__ ooff, int32_t *parent,
+                                  int32_t *queue, BfsCounters *cnt) {
+  const int src = inv[source_old];
+  parent[src] = src;
+  queue[0] = src;
+  cnt->qtail = 1;
+  cnt->scout = static_cast<unsigned long long>(out_degree(ooff, src));
+  cnt->awake = 0;
 }
 
-__global__ void bfs_init_kernel(int32_t n, const int32_t *__restrict__ ooff, int src,
-                                int32_t *parent, int32_t *queue) {
-  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride) {
-    const int32_t d = out_degree(ooff, static_cast<int>(v));
-    parent[v] = (v == src) ? src : (d != 0 ? -d : -1);
+// Block-wide append: every thread holds up to K flagged values (bit k of
+// `mask` set: vals[k] is appended).  One global atomic per block reserves
+// the block's run of the queue; the block's values land contiguously.  Must
+// be called by every thread of the block.
+template <int NT, int K>
+__device__ __forceinline__ void block_append(unsigned mask, const int (&vals)[K], int32_t *queue,
+                                             unsigned long long *tail, unsigned *s_warp,
+                                             unsigned long long *s_base) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned mine = __popc(mask);
+  unsigned incl = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) queue[0] = src;
+  if (lane == 31) s_warp[wid] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned tot = 0;
+    for (int w = 0; w < NT / 32; w++) {
+      const unsigned t = s_warp[w];
+      s_warp[w] = tot;
+      tot += t;
+    }
+    *s_base = tot ? atomicAdd(tail, static_cast<unsigned long long>(tot)) : 0ull;
+  }
+  __syncthreads();
+  unsigned long long pos = *s_base + s_warp[wid] + (incl - mine);
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if ((mask >> k) & 1u) queue[pos++] = vals[k];
+  __syncthreads();  // s_warp / s_base are reused by the next call
 }
 
 // Out-degree of every frontier vertex (input of the edge scan).
@@ -85,37 +110,91 @@ __global__ void bfs_frontier_degree_kernel(int64_t q, const int32_t *__restrict_
 }
 
 // Top-down step over the frontier's edges: edge e belongs to the frontier
-// vertex i with eoff[i] <= e < eoff[i + 1] (eoff: exclusive scan of degrees).
-__global__ void bfs_td_kernel(int64_t q, const int32_t *__restrict__ queue,
-                              const int64_t *__restrict__ eoff, const int32_t *__restrict__ ooff,
-                              const int32_t *__restrict__ onbr, int32_t *parent, int32_t *next,
-                              BfsCounters *cnt) {
-  const int64_t edges = eoff[q];  // the scan's total: no host round trip
-  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  unsigned long long scout = 0;
-  const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  // whole warps iterate together so the appends can use warp ballots
-  const int64_t rounds = (edges + stride - 1) / stride;
-  for (int64_t r = 0; r < rounds; r++) {
-    const int64_t e = first + r * stride;
-    bool claimed = false;
-    int v = 0;
-    if (e < edges) {
-      int64_t lo = 0, hi = q - 1;  // last i with eoff[i] <= e
-      while (lo < hi) {
-        const int64_t mid = (lo + hi + 1) >> 1;
-        if (eoff[mid] <= e) lo = mid;
-        else hi = mid - 1;
+// vertex i with eoff[i] <= e < eoff[i + 1] (eoff: exclusive scan of the
+// frontier's out-degrees, eoff[q] = edges).  Each block takes chunks of
+// NT * PT consecutive edges; a thread's edges are NT apart, so its
+// frontier index only moves forward and is re-searched only when it passes
+// the current vertex.  SMALL (q <= NT): every block scans the frontier's
+// degrees itself in shared memory, so a small step is one launch.
+template <int NT, int PT, bool SMALL>
+__global__ void __launch_bounds__(NT)
+bfs_td_kernel(int64_t q, const int32_t *__restrict__ queue_g, const int64_t *__restrict__ eoff_g,
+              const int32_t *__restrict__ ooff, const int32_t *__restrict__ onbr,
+              int32_t *parent, int32_t *next, BfsCounters *cnt) {
+  __shared__ int64_t s_eoff[SMALL ? NT + 1 : 1];
+  __shared__ int32_t s_q[SMALL ? NT : 1];
+  __shared__ unsigned s_warp[NT / 32];
+  __shared__ unsigned long long s_base;
+  const int64_t *eoff = eoff_g;
+  const int32_t *queue = queue_g;
+  if (SMALL) {
+    // exclusive scan of the frontier's out-degrees: warp scans, then the
+    // warp totals (s_eoff[NT] ends as the edge count)
+    __shared__ int64_t s_wsum[NT / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int32_t u = 0;
+    int64_t d = 0;
+    if (threadIdx.x < q) {
+      u = queue_g[threadIdx.x];
+      d = out_degree(ooff, u);
+    }
+    int64_t incl = d;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_wsum[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int64_t run = 0;
+      for (int w = 0; w < NT / 32; w++) {
+        const int64_t t = s_wsum[w];
+        s_wsum[w] = run;
+        run += t;
       }
-      const int u = queue[lo];
-      v = onbr[ooff[u] + (e - eoff[lo])];
-      const int32_t cur = *reinterpret_cast<volatile int32_t *>(parent + v);
-      if (cur < 0 && atomicCAS(parent + v, cur, u) == cur) {
-        claimed = true;
-        scout += static_cast<unsigned long long>(-cur);
+      s_eoff[NT] = run;
+    }
+    __syncthreads();
+    s_eoff[threadIdx.x] = s_wsum[wid] + incl - d;
+    s_q[threadIdx.x] = u;
+    __syncthreads();
+    eoff = s_eoff;
+    queue = s_q;
+  }
+  const int64_t edges = eoff[q];  // the scan's total: no host round trip
+  constexpr int64_t kChunk = static_cast<int64_t>(NT) * PT;
+  unsigned long long scout = 0;
+  int64_t lo = 0;  // frontier index of this thread's previous edge
+  for (int64_t c0 = static_cast<int64_t>(blockIdx.x) * kChunk; c0 < edges;
+       c0 += static_cast<int64_t>(gridDim.x) * kChunk) {
+    int vals[PT];
+    unsigned mask = 0;
+#pragma unroll
+    for (int k = 0; k < PT; k++) {
+      const int64_t e = c0 + k * NT + threadIdx.x;
+      vals[k] = 0;
+      if (e < edges) {
+        if (eoff[lo + 1] <= e) {  // past vertex lo: last i with eoff[i] <= e
+          int64_t l = lo + 1, h = q - 1;
+          while (l < h) {
+            const int64_t mid = (l + h + 1) >> 1;
+            if (eoff[mid] <= e) l = mid;
+            else h = mid - 1;
+          }
+          lo = l;
+        }
+        const int u = queue[lo];
+        const int v = onbr[ooff[u] + (e - eoff[lo])];
+        const int32_t cur = *reinterpret_cast<volatile int32_t *>(parent + v);
+        if (cur < 0 && atomicCAS(parent + v, cur, u) == cur) {
+          vals[k] = v;
+          mask |= 1u << k;
+          scout += static_cast<unsigned long long>(max(out_degree(ooff, v), 1));
+        }
       }
     }
-    warp_append(claimed, v, next, &cnt->qtail);
+    block_append<NT, PT>(mask, vals, next, &cnt->qtail, s_warp, &s_base);
   }
   for (int o = 16; o > 0; o >>= 1) scout += __shfl_xor_sync(0xffffffffu, scout, o);
   if ((threadIdx.x & 31) == 0 && scout) atomicAdd(&cnt->scout, scout);
@@ -130,10 +209,17 @@ __global__ void bfs_queue_to_bitmap_kernel(int64_t q, const int32_t *__restrict_
   }
 }
 
+__device__ __forceinline__ bool in_front(const unsigned *__restrict__ front, int u) {
+  return (__ldg(front + (u >> 5)) >> (u & 31)) & 1u;
+}
+
 // Bottom-up step: each warp owns 32 consecutive vertices (one bitmap word).
-__global__ void bfs_bu_kernel(int32_t n, const int32_t *__restrict__ ioff,
+// Only rows [0, rows) have in-neighbours (rows are sorted by in-degree), so
+// only their words are visited; the words after them stay zero.
+__global__ void bfs_bu_kernel(int32_t rows, const int32_t *__restrict__ ioff,
                               const int32_t *__restrict__ inbr, const unsigned *__restrict__ front,
                               unsigned *next, int32_t *parent, BfsCounters *cnt) {
+  const int32_t n = rows;
   const int lane = threadIdx.x & 31;
   const int64_t words = (static_cast<int64_t>(n) + 31) >> 5;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
@@ -145,7 +231,7 @@ __global__ void bfs_bu_kernel(int32_t n, const int32_t *__restrict__ ioff,
     if (v < n && parent[v] < 0) {
       for (int j = ioff[v]; j < ioff[v + 1]; j++) {
         const int u = inbr[j];
-        if ((__ldg(front + (u >> 5)) >> (u & 31)) & 1u) {
+        if (in_front(front, u)) {
           parent[v] = u;
           found = true;
           break;
@@ -160,16 +246,53 @@ __global__ void bfs_bu_kernel(int32_t n, const int32_t *__restrict__ ioff,
   if (lane == 0 && awake) atomicAdd(&cnt->awake, awake);
 }
 
-__global__ void bfs_bitmap_to_queue_kernel(int32_t n, const unsigned *__restrict__ bm,
-                                           int32_t *queue, BfsCounters *cnt) {
-  const int lane = threadIdx.x & 31;
+// Set bits of the bitmap -> queue, over the words of vertices [0, n).  Each
+// thread takes one word per block round and appends its vertices (up to 32)
+// with one global atomic per block round.
+constexpr int kB2qThreads = 256;
+
+__global__ void __launch_bounds__(kB2qThreads)
+bfs_bitmap_to_queue_kernel(int32_t n, const unsigned *__restrict__ bm, int32_t *queue,
+                           BfsCounters *cnt) {
+  __shared__ unsigned s_warp[kB2qThreads / 32];
+  __shared__ unsigned long long s_base;
   const int64_t words = (static_cast<int64_t>(n) + 31) >> 5;
-  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; w < words;
-       w += warps) {
-    const unsigned word = bm[w];  // same value in every lane
-    const int64_t v = (w << 5) + lane;
-    warp_append(((word >> lane) & 1u) != 0u && v < n, static_cast<int>(v), queue, &cnt->qtail);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int64_t w0 = static_cast<int64_t>(blockIdx.x) * kB2qThreads; w0 < words;
+       w0 += static_cast<int64_t>(gridDim.x) * kB2qThreads) {
+    const int64_t w = w0 + threadIdx.x;
+    unsigned word = 0;
+    if (w < words) {
+      word = bm[w];
+      const int64_t rest = static_cast<int64_t>(n) - (w << 5);
+      if (rest < 32) word &= (1u << rest) - 1u;
+    }
+    const unsigned mine = __popc(word);
+    unsigned incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned tot = 0;
+      for (int k = 0; k < kB2qThreads / 32; k++) {
+        const unsigned t = s_warp[k];
+        s_warp[k] = tot;
+        tot += t;
+      }
+      s_base = tot ? atomicAdd(&cnt->qtail, static_cast<unsigned long long>(tot)) : 0ull;
+    }
+    __syncthreads();
+    unsigned long long pos = s_base + s_warp[wid] + (incl - mine);
+    while (word) {
+      const int b = __ffs(word) - 1;
+      word &= word - 1u;
+      queue[pos++] = static_cast<int32_t>((w << 5) + b);
+    }
+    __syncthreads();
   }
 }
 
@@ -185,11 +308,29 @@ __global__ void bfs_finish_kernel(int32_t n, const int32_t *__restrict__ parent,
   }
 }
 
-unsigned BfsGrid(int64_t items) {
+int NumSms() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((items + 255) / 256, sms * 16)));
+  return sms;
+}
+
+unsigned BfsGrid(int64_t items) {
+  return static_cast<unsigned>(
+      std::max<int64_t>(1, std::min<int64_t>((items + 255) / 256, NumSms() * 16)));
+}
+
+// top-down blocks: threads and edges per thread per chunk, with the
+// frontier scanned by CUB, or scanned by each block itself (small frontiers)
+constexpr int kTdThreads = 256, kTdPerThread = 8;
+constexpr int kTdSmallThreads = 1024, kTdSmallPerThread = 4;
+
+// Blocks for a top-down step of at most `edges` edges: one chunk each, at
+// most two resident waves.
+unsigned TdGrid(int64_t edges, int threads, int per_thread) {
+  const int64_t chunk = static_cast<int64_t>(threads) * per_thread;
+  const int64_t cap = static_cast<int64_t>(NumSms()) * (4096 / threads);
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((edges + chunk - 1) / chunk, cap)));
 }
 
 }  // namespace
@@ -221,6 +362,10 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
   const int32_t *onbr = g.directed ? g.ocol : g.col;
   const int32_t *ioff = g.rowoff;
   const int32_t *inbr = g.col;
+  // in-CSR rows with in-neighbours (rows are sorted by in-degree; the rest
+  // can only be reached as the source)
+  const int32_t in_rows = static_cast<int32_t>(g.bin_row_start[kBinZero]);
+  const int64_t in_words = (static_cast<int64_t>(in_rows) + 31) / 32;
   if (!b.parent || b.cap_n < n) {
     FreeBfsScratch(&b);
     BFS_TRY(cudaMalloc(&b.parent, sizeof(int32_t) * std::max<int64_t>(n, 1)));
@@ -252,28 +397,24 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
   auto record = [&](const char *kind, int64_t count, double sec) {
     if (steps) steps->push_back(BfsStep{kind, count, sec});
   };
-  auto t0 = clock::now();
-  int32_t src = 0;
-  BFS_TRY(cudaMemcpyAsync(&src, g.inv + source_old, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  BFS_TRY(cudaStreamSynchronize(s));
-  const unsigned grid = BfsGrid(n);
-  bfs_init_kernel<<<grid, 256, 0, s>>>(static_cast<int32_t>(n), ooff, src, b.parent, b.queue[0]);
-  BFS_TRY(cudaGetLastError());
-  int32_t src_off[2] = {0, 0};
-  BFS_TRY(cudaMemcpyAsync(src_off, ooff + src, sizeof(src_off), cudaMemcpyDeviceToHost, s));
-  BFS_TRY(cudaStreamSynchronize(s));
-  record("i", -1, seconds(t0, clock::now()));
-
   BfsCounters hc{};
   auto read_counters = [&]() -> cudaError_t {
     cudaError_t e = cudaMemcpyAsync(&hc, b.cnt, sizeof(hc), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     return e;
   };
+  auto t0 = clock::now();
+  const unsigned grid = BfsGrid(n);
+  BFS_TRY(cudaMemsetAsync(b.parent, 0xff, sizeof(int32_t) * n, s));  // every parent -1
+  bfs_source_kernel<<<1, 1, 0, s>>>(g.inv, source_old, ooff, b.parent, b.queue[0], cnt);
+  BFS_TRY(cudaGetLastError());
+  BFS_TRY(read_counters());
+  record("i", -1, seconds(t0, clock::now()));
+
   int cur = 0;                // queue[cur] is the frontier
   int64_t qsize = 1;
   int64_t edges_to_check = g.m;
-  int64_t scout_count = src_off[1] - src_off[0];
+  int64_t scout_count = static_cast<int64_t>(hc.scout);
   // every step reaches at least one new vertex, so n + 2 steps bound the
   // search; the guard turns a defect into an error instead of a host loop
   int64_t guard = 0;
@@ -285,9 +426,10 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
     if (scout_count > edges_to_check / alpha) {
       auto ts = clock::now();
       BFS_TRY(cudaMemsetAsync(b.bm[0], 0, sizeof(unsigned) * words, s));
+      BFS_TRY(cudaMemsetAsync(b.bm[1], 0, sizeof(unsigned) * words, s));
       bfs_queue_to_bitmap_kernel<<<BfsGrid(qsize), 256, 0, s>>>(qsize, b.queue[cur], b.bm[0]);
       BFS_TRY(cudaGetLastError());
-      BFS_TRY(cudaStreamSynchronize(s));
+      if (steps) BFS_TRY(cudaStreamSynchronize(s));  // only to time the step
       record("e", -1, seconds(ts, clock::now()));
       int front = 0;
       int64_t awake = qsize, old_awake = 0;
@@ -295,10 +437,12 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
         ts = clock::now();
         old_awake = awake;
         BFS_TRY(cudaMemsetAsync(b.cnt, 0, sizeof(BfsCounters), s));
-        bfs_bu_kernel<<<BfsGrid(words * 32), 256, 0, s>>>(static_cast<int32_t>(n), ioff, inbr,
-                                                          b.bm[front], b.bm[front ^ 1], b.parent,
-                                                          cnt);
+        bfs_bu_kernel<<<BfsGrid(in_rows), 256, 0, s>>>(in_rows, ioff, inbr, b.bm[front],
+                                                       b.bm[front ^ 1], b.parent, cnt);
         BFS_TRY(cudaGetLastError());
+        if (front == 0 && in_words < words)  // the frontier's bits past in_rows (a source
+          BFS_TRY(cudaMemsetAsync(b.bm[0] + in_words, 0,  // without in-edges) are spent
+                                  sizeof(unsigned) * (words - in_words), s));
         BFS_TRY(read_counters());
         awake = static_cast<int64_t>(hc.awake);
         front ^= 1;
@@ -310,8 +454,9 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
       } while (awake >= old_awake || awake > n / beta);
       ts = clock::now();
       BFS_TRY(cudaMemsetAsync(b.cnt, 0, sizeof(BfsCounters), s));
-      bfs_bitmap_to_queue_kernel<<<BfsGrid(words * 32), 256, 0, s>>>(
-          static_cast<int32_t>(n), b.bm[front], b.queue[cur], cnt);
+      // the last bottom-up step wrote the words of rows [0, in_rows) only
+      bfs_bitmap_to_queue_kernel<<<BfsGrid(in_rows), kB2qThreads, 0, s>>>(
+          in_rows, b.bm[front], b.queue[cur], cnt);
       BFS_TRY(cudaGetLastError());
       BFS_TRY(read_counters());
       qsize = static_cast<int64_t>(hc.qtail);
@@ -320,16 +465,27 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
     } else {
       auto ts = clock::now();
       edges_to_check -= scout_count;
-      bfs_frontier_degree_kernel<<<BfsGrid(qsize), 256, 0, s>>>(qsize, b.queue[cur], ooff, b.deg);
-      BFS_TRY(cudaGetLastError());
-      BFS_TRY(cudaMemsetAsync(b.deg + qsize, 0, sizeof(int64_t), s));
-      size_t bytes = static_cast<size_t>(b.cap_tmp);
-      BFS_TRY(cub::DeviceScan::ExclusiveSum(b.tmp, bytes, b.deg, b.eoff, static_cast<int>(qsize + 1),
-                                            s));
-      BFS_TRY(cudaMemsetAsync(b.cnt, 0, sizeof(BfsCounters), s));
-      // grid sized by the largest edge count the frontier can have
-      bfs_td_kernel<<<BfsGrid(std::min<int64_t>(g.m, qsize * g.max_degree)), 256, 0, s>>>(
-          qsize, b.queue[cur], b.eoff, ooff, onbr, b.parent, b.queue[cur ^ 1], cnt);
+      // grid sized by the largest edge count the frontier can have (the
+      // kernels loop over whatever the real count is)
+      const int64_t edge_bound = std::min<int64_t>(g.m, qsize * g.max_degree);
+      if (qsize <= kTdSmallThreads) {
+        BFS_TRY(cudaMemsetAsync(b.cnt, 0, sizeof(BfsCounters), s));
+        bfs_td_kernel<kTdSmallThreads, kTdSmallPerThread, true>
+            <<<TdGrid(edge_bound, kTdSmallThreads, kTdSmallPerThread), kTdSmallThreads, 0, s>>>(
+                qsize, b.queue[cur], nullptr, ooff, onbr, b.parent, b.queue[cur ^ 1], cnt);
+      } else {
+        bfs_frontier_degree_kernel<<<BfsGrid(qsize), 256, 0, s>>>(qsize, b.queue[cur], ooff,
+                                                                  b.deg);
+        BFS_TRY(cudaGetLastError());
+        BFS_TRY(cudaMemsetAsync(b.deg + qsize, 0, sizeof(int64_t), s));
+        size_t bytes = static_cast<size_t>(b.cap_tmp);
+        BFS_TRY(cub::DeviceScan::ExclusiveSum(b.tmp, bytes, b.deg, b.eoff,
+                                              static_cast<int>(qsize + 1), s));
+        BFS_TRY(cudaMemsetAsync(b.cnt, 0, sizeof(BfsCounters), s));
+        bfs_td_kernel<kTdThreads, kTdPerThread, false>
+            <<<TdGrid(edge_bound, kTdThreads, kTdPerThread), kTdThreads, 0, s>>>(
+            qsize, b.queue[cur], b.eoff, ooff, onbr, b.parent, b.queue[cur ^ 1], cnt);
+      }
       BFS_TRY(cudaGetLastError());
       BFS_TRY(read_counters());
       scout_count = static_cast<int64_t>(hc.scout);
