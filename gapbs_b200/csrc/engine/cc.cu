@@ -9,7 +9,8 @@
 // exactly it:
 //   1. comp[v] = v;
 //   2. two sampling rounds: every vertex links with its r-th out-neighbour
-//      (r = 0, 1), each round followed by a compress;
+//      (r = 0, 1), each round followed by a compress (which keeps the next
+//      round's link chases short);
 //   3. the component of the highest-degree vertex (row 0 of the degree-sorted
 //      mirror: a vertex of the largest intermediate component, which the
 //      reference estimates by sampling) is skipped in the final phase; row 0
@@ -19,7 +20,8 @@
 //      directed graph, with all its in-neighbours; compress;
 //   5. ids are mapped back: each root takes the smallest original id of its
 //      component (atomicMin; the largest component's members reduced per
-//      block first), every vertex that root's label.
+//      block first), every vertex that root's label; a vertex without edges
+//      is its own component and keeps its own id.
 // Link is the reference's lock-free hooking loop with compare-and-swap; it
 // and the compress chase are bounded (an iteration limit sets an error flag
 // instead of spinning), so a defect cannot hang the device.
@@ -66,7 +68,8 @@ __global__ void cc_init_kernel(int32_t n, int *comp) {
     comp[v] = static_cast<int>(v);
 }
 
-// One sampling round: vertex u links with its r-th out-neighbour.
+// One sampling round (src/cc.cc:100-106): vertex u links with its r-th
+// out-neighbour.
 __global__ void cc_sample_kernel(int32_t n, const int32_t *__restrict__ off,
                                  const int32_t *__restrict__ nbr, int r, int *comp, int *err) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -160,11 +163,16 @@ __global__ void __launch_bounds__(256) cc_root_min_kernel(int32_t n, const int *
   }
 }
 
-__global__ void cc_label_kernel(int32_t n, const int *comp, const int32_t *__restrict__ perm,
-                                const int *root_min, int32_t *out_old) {
+// Label of every original id o (a gather, so the writes are coalesced):
+// rows [active, n) have no edges and are their own components.
+__global__ void cc_label_kernel(int32_t n, int32_t active, const int *comp,
+                                const int32_t *__restrict__ inv, const int *root_min,
+                                int32_t *out_old) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride)
-    out_old[perm[v]] = root_min[comp[v]];
+  for (int64_t o = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; o < n; o += stride) {
+    const int v = inv[o];
+    out_old[o] = v < active ? root_min[comp[v]] : static_cast<int32_t>(o);
+  }
 }
 
 __global__ void fill_kernel(int32_t n, int value, int *a) {
@@ -220,10 +228,10 @@ cudaError_t ConnectedComponents(const DeviceGraph &g, CcScratch &cs, cudaStream_
   // rows of at least 32 entries (the front of the mirror) take a warp each
   const int32_t long_rows = std::min<int32_t>(active, static_cast<int32_t>(g.bin_row_start[4]));
   if (e == cudaSuccess) {
-    cc_init_kernel<<<grid, 256, 0, s>>>(n, comp);
+    cc_init_kernel<<<CcGrid(active), 256, 0, s>>>(active, comp);
     for (int r = 0; r < kRounds; r++) {
-      cc_sample_kernel<<<grid, 256, 0, s>>>(active, ooff, onbr, r, comp, derr);
-      cc_compress_kernel<<<grid, 256, 0, s>>>(active, comp, derr);
+      cc_sample_kernel<<<CcGrid(active), 256, 0, s>>>(active, ooff, onbr, r, comp, derr);
+      cc_compress_kernel<<<CcGrid(active), 256, 0, s>>>(active, comp, derr);
     }
     e = cudaGetLastError();
   }
@@ -237,10 +245,11 @@ cudaError_t ConnectedComponents(const DeviceGraph &g, CcScratch &cs, cudaStream_
     if (active > long_rows)
       cc_finish_thread_kernel<<<CcGrid(active - long_rows), 256, 0, s>>>(
           long_rows, active, ooff, onbr, ioff, inbr, kRounds, giant, comp, derr);
-    cc_compress_kernel<<<grid, 256, 0, s>>>(active, comp, derr);
-    fill_kernel<<<grid, 256, 0, s>>>(n, INT_MAX, root_min);
-    cc_root_min_kernel<<<grid, 256, 0, s>>>(n, comp, g.perm, root_min);
-    cc_label_kernel<<<grid, 256, 0, s>>>(n, comp, g.perm, root_min, out_old);
+    // roots of the rows [0, active) are rows of [0, active)
+    cc_compress_kernel<<<CcGrid(active), 256, 0, s>>>(active, comp, derr);
+    fill_kernel<<<CcGrid(active), 256, 0, s>>>(active, INT_MAX, root_min);
+    cc_root_min_kernel<<<CcGrid(active), 256, 0, s>>>(active, comp, g.perm, root_min);
+    cc_label_kernel<<<grid, 256, 0, s>>>(n, active, comp, g.inv, root_min, out_old);
     e = cudaGetLastError();
   }
   int herr = 0;
