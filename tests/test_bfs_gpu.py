@@ -94,3 +94,46 @@ def test_generated_graph_and_errors(engine):
         engine.bfs(-1)
     with pytest.raises(PageRankError):
         engine.bfs(engine.n)
+
+
+def layered(widths, rng, extra=1):
+    """Source 0, then layers of the given widths; every vertex of a layer has
+    one edge from a random vertex of the layer before, plus `extra` more."""
+    us, vs = [], []
+    prev = np.array([0])
+    nxt = 1
+    for w in widths:
+        layer = np.arange(nxt, nxt + w)
+        nxt += w
+        for _ in range(1 + extra):
+            us.append(rng.choice(prev, w))
+            vs.append(layer)
+        prev = layer
+    return np.concatenate(us), np.concatenate(vs)
+
+
+@pytest.mark.parametrize("widths", [(1023, 2000, 7), (1024, 1025, 3), (1025, 5000, 40, 1),
+                                    (3000, 1024, 1023, 2)])
+def test_frontier_sizes_around_block_scan(engine, widths):
+    # top-down frontiers of up to 1,024 vertices are scanned inside each block,
+    # larger ones by a device-wide scan: both sides of the boundary
+    rng = np.random.default_rng(sum(widths))
+    u, v = layered(widths, rng)
+    for sym in (True, False):
+        g = Graph.from_edges(u, v, symmetrize=sym)
+        engine.upload(g)
+        check(g, 0, engine.bfs(0))
+
+
+def test_directed_source_without_in_edges(engine):
+    # the source has out-edges only (it sorts after every row with in-edges)
+    # and a large degree, so the search goes bottom-up from the first step and
+    # stays there for several steps
+    rng = np.random.default_rng(11)
+    u, v = layered((20000, 30000, 30000, 500, 20), rng, extra=2)
+    g = Graph.from_edges(u, v, symmetrize=False)
+    engine.upload(g)
+    parent, steps = engine.bfs(0, with_steps=True)
+    check(g, 0, parent)
+    kinds = [k for k, _, _ in steps]
+    assert kinds[1] == "e" and kinds.count("bu") >= 3
