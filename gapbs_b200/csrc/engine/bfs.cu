@@ -296,15 +296,25 @@ bfs_bitmap_to_queue_kernel(int32_t n, const unsigned *__restrict__ bm, int32_t *
   }
 }
 
-// parent < -1 -> -1, in original ids: each original id gathers its row's
-// parent (coalesced writes; a scatter through perm wrote partial sectors).
-__global__ void bfs_finish_kernel(int32_t n, const int32_t *__restrict__ parent,
+// Parents in original ids, -1 for unreached: each original id gathers its
+// row's parent (coalesced writes; a scatter through perm wrote partial
+// sectors).  Rows [in_rows, n) have no in-edges, so only the source among
+// them is reached; their parents are not read.
+__global__ void bfs_finish_kernel(int32_t n, int32_t in_rows, int source_old,
+                                  const int32_t *__restrict__ parent,
                                   const int32_t *__restrict__ perm,
                                   const int32_t *__restrict__ inv, int32_t *out_old) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride) {
-    const int32_t p = parent[inv[v]];
-    out_old[v] = p >= 0 ? perm[p] : -1;
+  for (int64_t o = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; o < n; o += stride) {
+    const int v = inv[o];
+    int32_t r = -1;
+    if (v < in_rows) {
+      const int32_t p = parent[v];
+      if (p >= 0) r = perm[p];
+    } else if (o == source_old) {
+      r = source_old;
+    }
+    out_old[o] = r;
   }
 }
 
@@ -494,7 +504,8 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
       record("td", qsize, seconds(ts, clock::now()));
     }
   }
-  bfs_finish_kernel<<<grid, 256, 0, s>>>(static_cast<int32_t>(n), b.parent, g.perm, g.inv,
+  bfs_finish_kernel<<<grid, 256, 0, s>>>(static_cast<int32_t>(n), in_rows, source_old, b.parent,
+                                         g.perm, g.inv,
                                          out_old);
   BFS_TRY(cudaGetLastError());
   BFS_TRY(cudaStreamSynchronize(s));

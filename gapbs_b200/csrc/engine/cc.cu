@@ -44,10 +44,22 @@ __device__ __forceinline__ int ld_comp(const int *comp, int x) {
   return *reinterpret_cast<const volatile int *>(comp + x);
 }
 
-// src/cc.cc:40-55 with compare-and-swap on the device.
+// A weak load that may be served from this SM's L1 and so be stale.  Used
+// where any ancestor of x serves as well as its current parent: comp values
+// only ever move to other members of the same tree, and a root stays a root
+// until a link hooks it.  Most chases end at the few roots of the largest
+// components, whose lines would otherwise be requested from L2 by every warp.
+__device__ __forceinline__ int ld_comp_cached(const int *comp, int x) {
+  int r;
+  asm volatile("ld.global.ca.s32 %0, [%1];" : "=r"(r) : "l"(comp + x));
+  return r;
+}
+
+// src/cc.cc:40-55 with compare-and-swap on the device.  p2 may be any member
+// of v's tree (the loop re-reads before every decision).
 __device__ void cc_link(int u, int v, int *comp, int *err) {
   int p1 = ld_comp(comp, u);
-  int p2 = ld_comp(comp, v);
+  int p2 = ld_comp_cached(comp, v);
   for (int it = 0; p1 != p2; it++) {
     if (it >= kChaseLimit) {
       atomicExch(err, 1);
@@ -79,13 +91,15 @@ __global__ void cc_sample_kernel(int32_t n, const int32_t *__restrict__ off,
   }
 }
 
-// src/cc.cc:58-66
+// src/cc.cc:58-66.  No link runs during a compress, so roots are fixed and
+// every non-root x has comp[x] != x at all times: c == comp[c] holds exactly
+// when c is a root, whether comp[c] was read fresh or from L1.
 __global__ void cc_compress_kernel(int32_t n, int *comp, int *err) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride) {
     int it = 0;
     int c = ld_comp(comp, static_cast<int>(v));
-    int cc = ld_comp(comp, c);
+    int cc = ld_comp_cached(comp, c);
     while (c != cc) {
       if (++it >= kChaseLimit) {
         atomicExch(err, 1);
@@ -93,7 +107,7 @@ __global__ void cc_compress_kernel(int32_t n, int *comp, int *err) {
       }
       comp[v] = cc;
       c = cc;
-      cc = ld_comp(comp, c);
+      cc = ld_comp_cached(comp, c);
     }
   }
 }
@@ -171,7 +185,8 @@ __global__ void cc_label_kernel(int32_t n, int32_t active, const int *comp,
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t o = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; o < n; o += stride) {
     const int v = inv[o];
-    out_old[o] = v < active ? root_min[comp[v]] : static_cast<int32_t>(o);
+    // comp and root_min are final here (read-only path)
+    out_old[o] = v < active ? __ldg(root_min + __ldg(comp + v)) : static_cast<int32_t>(o);
   }
 }
 
