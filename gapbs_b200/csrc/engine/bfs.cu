@@ -186,7 +186,11 @@ bfs_td_kernel(int64_t q, const int32_t *__restrict__ queue_g, const int64_t *__r
         }
         const int u = queue[lo];
         const int v = onbr[ooff[u] + (e - eoff[lo])];
-        const int32_t cur = *reinterpret_cast<volatile int32_t *>(parent + v);
+        // a weak load that L1 may serve (the popular targets are hubs read
+        // by every block): a parent never returns to -1, so a value >= 0 is
+        // final, and a stale -1 only costs a compare-and-swap that fails
+        int32_t cur;
+        asm volatile("ld.global.ca.s32 %0, [%1];" : "=r"(cur) : "l"(parent + v));
         if (cur < 0 && atomicCAS(parent + v, cur, u) == cur) {
           vals[k] = v;
           mask |= 1u << k;
