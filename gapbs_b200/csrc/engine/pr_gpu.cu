@@ -5,8 +5,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <thread>
@@ -63,24 +65,76 @@ int CudaErr(pr_gpu_t *h, cudaError_t e, const char *what) {
     if (e_ != cudaSuccess) return CudaErr((h), e_, #expr);  \
   } while (0)
 
-// Parallel memcpy for large host-to-host staging copies.
+// Parallel memcpy for the host-to-host staging copies: a process-wide pool of
+// worker threads, started once (a staging chunk is copied in well under a
+// millisecond, so starting threads per chunk would cost as much as the copy).
+// One copy runs at a time; the caller copies the first share itself.  The
+// pool is never destroyed: its idle workers end with the process.
+class CopyPool {
+ public:
+  static CopyPool &Get() {
+    static CopyPool *pool = new CopyPool();
+    return *pool;
+  }
+
+  void Copy(void *dst, const void *src, size_t bytes) {
+    std::lock_guard<std::mutex> one_at_a_time(call_mu_);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      dst_ = static_cast<char *>(dst);
+      src_ = static_cast<const char *>(src);
+      bytes_ = bytes;
+      pending_ = nt_ - 1;
+      gen_++;
+    }
+    work_cv_.notify_all();
+    Share(0);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return pending_ == 0; });
+  }
+
+ private:
+  CopyPool()
+      : nt_(static_cast<int>(std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2)))) {
+    for (int t = 1; t < nt_; t++) std::thread([this, t] { Worker(t); }).detach();
+  }
+
+  void Share(int t) const {
+    const size_t per = (bytes_ + nt_ - 1) / nt_;
+    const size_t lo = std::min(bytes_, per * t), hi = std::min(bytes_, per * (t + 1));
+    if (hi > lo) std::memcpy(dst_ + lo, src_ + lo, hi - lo);
+  }
+
+  void Worker(int t) {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        work_cv_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+      }
+      Share(t);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--pending_ == 0) done_cv_.notify_one();
+    }
+  }
+
+  const int nt_;
+  std::mutex call_mu_, mu_;
+  std::condition_variable work_cv_, done_cv_;
+  uint64_t gen_ = 0;
+  int pending_ = 0;
+  char *dst_ = nullptr;
+  const char *src_ = nullptr;
+  size_t bytes_ = 0;
+};
+
 void HostCopy(void *dst, const void *src, size_t bytes) {
-  const size_t kPar = 8u << 20;
-  if (bytes < kPar) {
+  if (bytes < (size_t(8) << 20)) {
     std::memcpy(dst, src, bytes);
     return;
   }
-  static const int nt = static_cast<int>(
-      std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2)));
-  std::thread th[8];
-  const size_t per = (bytes + nt - 1) / nt;
-  for (int t = 0; t < nt; t++) {
-    const size_t lo = std::min(bytes, per * t), hi = std::min(bytes, per * (t + 1));
-    th[t] = std::thread([=] {
-      std::memcpy(static_cast<char *>(dst) + lo, static_cast<const char *>(src) + lo, hi - lo);
-    });
-  }
-  for (int t = 0; t < nt; t++) th[t].join();
+  CopyPool::Get().Copy(dst, src, bytes);
 }
 
 void FreeGenerated(pr_gpu_t *h) {
