@@ -55,8 +55,16 @@ __device__ __forceinline__ int ld_comp_cached(const int *comp, int x) {
   return r;
 }
 
-// src/cc.cc:40-55 with compare-and-swap on the device.  p2 may be any member
-// of v's tree (the loop re-reads before every decision).
+// src/cc.cc:40-55 with compare-and-swap on the device.  Reads that may come
+// from L1 (stale) are safe here: a stale comp[x] is x itself or one of x's
+// ancestors, a vertex that is not a root never becomes one again, and
+// comp[high] == low at any time means high and low share a tree for good.
+// A value that looks like a root is confirmed from L2 before the
+// compare-and-swap, and a failed compare-and-swap returns the current
+// parent.  Every pass of the loop moves high strictly up its tree, so the
+// loop ends; the iteration limit only guards against a defect.  The roots
+// of the large trees are read by almost every warp in the second sampling
+// round, which is what keeps those reads in L1.
 __device__ void cc_link(int u, int v, int *comp, int *err) {
   int p1 = ld_comp(comp, u);
   int p2 = ld_comp_cached(comp, v);
@@ -66,11 +74,18 @@ __device__ void cc_link(int u, int v, int *comp, int *err) {
       return;
     }
     const int high = max(p1, p2), low = min(p1, p2);
-    const int p_high = ld_comp(comp, high);
+    int p_high = ld_comp_cached(comp, high);
+    if (p_high == high) {
+      p_high = ld_comp(comp, high);
+      if (p_high == high) {
+        const int old = atomicCAS(comp + high, high, low);
+        if (old == high) return;
+        p_high = old;
+      }
+    }
     if (p_high == low) return;
-    if (p_high == high && atomicCAS(comp + high, high, low) == high) return;
-    p1 = ld_comp(comp, ld_comp(comp, high));
-    p2 = ld_comp(comp, low);
+    p1 = ld_comp_cached(comp, p_high);  // at or above high's parent
+    p2 = ld_comp_cached(comp, low);
   }
 }
 
