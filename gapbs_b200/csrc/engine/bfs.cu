@@ -19,7 +19,9 @@
 //     then back to a queue (alpha = 15, beta = 18);
 //   * unvisited vertices end with parent -1.
 // The host drives the steps (one small read-back per step for the counts);
-// ids are the mirror's degree-sorted ids and are mapped back at the end.
+// queues and bitmaps hold the mirror's degree-sorted ids; parent[] is indexed
+// by mirror row but stores the parent's original id, so the write-back only
+// gathers it into original order.
 // Parents can differ from run to run (which frontier vertex wins a claim is
 // a race, as in the reference); depths, reached sets and tree sizes cannot.
 //
@@ -54,12 +56,14 @@ __device__ __forceinline__ int32_t out_degree(const int32_t *ooff, int v) {
 }
 
 // The source (original id) becomes its own parent and the first frontier;
-// its out-degree is the first scout count.  One thread.
+// its out-degree is the first scout count.  One thread.  parent[] is indexed
+// by mirror row but holds original ids (only its sign is read during the
+// search), so the write-back needs no second lookup.
 __global__ void bfs_source_kernel(const int32_t *__restrict__ inv, int source_old,
                                   const int32_t *__restrict__ ooff, int32_t *parent,
                                   int32_t *queue, BfsCounters *cnt) {
   const int src = inv[source_old];
-  parent[src] = src;
+  parent[src] = source_old;
   queue[0] = src;
   cnt->qtail = 1;
   cnt->scout = static_cast<unsigned long long>(out_degree(ooff, src));
@@ -120,7 +124,8 @@ template <int NT, int PT, bool SMALL>
 __global__ void __launch_bounds__(NT)
 bfs_td_kernel(int64_t q, const int32_t *__restrict__ queue_g, const int64_t *__restrict__ eoff_g,
               const int32_t *__restrict__ ooff, const int32_t *__restrict__ onbr,
-              int32_t *parent, int32_t *next, BfsCounters *cnt) {
+              const int32_t *__restrict__ perm, int32_t *parent, int32_t *next,
+              BfsCounters *cnt) {
   __shared__ int64_t s_eoff[SMALL ? NT + 1 : 1];
   __shared__ int32_t s_q[SMALL ? NT : 1];
   __shared__ unsigned s_warp[NT / 32];
@@ -191,7 +196,7 @@ bfs_td_kernel(int64_t q, const int32_t *__restrict__ queue_g, const int64_t *__r
         // final, and a stale -1 only costs a compare-and-swap that fails
         int32_t cur;
         asm volatile("ld.global.ca.s32 %0, [%1];" : "=r"(cur) : "l"(parent + v));
-        if (cur < 0 && atomicCAS(parent + v, cur, u) == cur) {
+        if (cur < 0 && atomicCAS(parent + v, cur, __ldg(perm + u)) == cur) {
           vals[k] = v;
           mask |= 1u << k;
           scout += static_cast<unsigned long long>(max(out_degree(ooff, v), 1));
@@ -222,7 +227,8 @@ __device__ __forceinline__ bool in_front(const unsigned *__restrict__ front, int
 // only their words are visited; the words after them stay zero.
 __global__ void bfs_bu_kernel(int32_t rows, const int32_t *__restrict__ ioff,
                               const int32_t *__restrict__ inbr, const unsigned *__restrict__ front,
-                              unsigned *next, int32_t *parent, BfsCounters *cnt) {
+                              const int32_t *__restrict__ perm, unsigned *next, int32_t *parent,
+                              BfsCounters *cnt) {
   const int32_t n = rows;
   const int lane = threadIdx.x & 31;
   const int64_t words = (static_cast<int64_t>(n) + 31) >> 5;
@@ -236,7 +242,7 @@ __global__ void bfs_bu_kernel(int32_t rows, const int32_t *__restrict__ ioff,
       for (int j = ioff[v]; j < ioff[v + 1]; j++) {
         const int u = inbr[j];
         if (in_front(front, u)) {
-          parent[v] = u;
+          parent[v] = __ldg(perm + u);
           found = true;
           break;
         }
@@ -306,15 +312,13 @@ bfs_bitmap_to_queue_kernel(int32_t n, const unsigned *__restrict__ bm, int32_t *
 // them is reached; their parents are not read.
 __global__ void bfs_finish_kernel(int32_t n, int32_t in_rows, int source_old,
                                   const int32_t *__restrict__ parent,
-                                  const int32_t *__restrict__ perm,
                                   const int32_t *__restrict__ inv, int32_t *out_old) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t o = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; o < n; o += stride) {
     const int v = inv[o];
     int32_t r = -1;
     if (v < in_rows) {
-      const int32_t p = parent[v];
-      if (p >= 0) r = perm[p];
+      r = parent[v];
     } else if (o == source_old) {
       r = source_old;
     }
@@ -451,7 +455,7 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
         ts = clock::now();
         old_awake = awake;
         BFS_TRY(cudaMemsetAsync(b.cnt, 0, sizeof(BfsCounters), s));
-        bfs_bu_kernel<<<BfsGrid(in_rows), 256, 0, s>>>(in_rows, ioff, inbr, b.bm[front],
+        bfs_bu_kernel<<<BfsGrid(in_rows), 256, 0, s>>>(in_rows, ioff, inbr, b.bm[front], g.perm,
                                                        b.bm[front ^ 1], b.parent, cnt);
         BFS_TRY(cudaGetLastError());
         if (front == 0 && in_words < words)  // the frontier's bits past in_rows (a source
@@ -486,7 +490,8 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
         BFS_TRY(cudaMemsetAsync(b.cnt, 0, sizeof(BfsCounters), s));
         bfs_td_kernel<kTdSmallThreads, kTdSmallPerThread, true>
             <<<TdGrid(edge_bound, kTdSmallThreads, kTdSmallPerThread), kTdSmallThreads, 0, s>>>(
-                qsize, b.queue[cur], nullptr, ooff, onbr, b.parent, b.queue[cur ^ 1], cnt);
+                qsize, b.queue[cur], nullptr, ooff, onbr, g.perm, b.parent, b.queue[cur ^ 1],
+                cnt);
       } else {
         bfs_frontier_degree_kernel<<<BfsGrid(qsize), 256, 0, s>>>(qsize, b.queue[cur], ooff,
                                                                   b.deg);
@@ -498,7 +503,7 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
         BFS_TRY(cudaMemsetAsync(b.cnt, 0, sizeof(BfsCounters), s));
         bfs_td_kernel<kTdThreads, kTdPerThread, false>
             <<<TdGrid(edge_bound, kTdThreads, kTdPerThread), kTdThreads, 0, s>>>(
-            qsize, b.queue[cur], b.eoff, ooff, onbr, b.parent, b.queue[cur ^ 1], cnt);
+            qsize, b.queue[cur], b.eoff, ooff, onbr, g.perm, b.parent, b.queue[cur ^ 1], cnt);
       }
       BFS_TRY(cudaGetLastError());
       BFS_TRY(read_counters());
@@ -509,8 +514,7 @@ cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t
     }
   }
   bfs_finish_kernel<<<grid, 256, 0, s>>>(static_cast<int32_t>(n), in_rows, source_old, b.parent,
-                                         g.perm, g.inv,
-                                         out_old);
+                                         g.inv, out_old);
   BFS_TRY(cudaGetLastError());
   BFS_TRY(cudaStreamSynchronize(s));
   return cudaSuccess;
