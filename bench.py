@@ -387,8 +387,8 @@ def run_ours(a, dist: Dist):
         bfs_ms = dist.max(t_total * 1e3 / max(1, len(picked)))
         bfs = {"workload": f"direction-optimizing BFS of {a.graph.strip()} from {len(picked)} "
                            "sources with out-edges (seeded draw)",
-               "ms": round(bfs_ms, 3), "unit": "ms per search (device-resident graph, host-"
-                                               "driven steps)",
+               "ms": round(bfs_ms, 3), "unit": "ms per search (device-resident graph, one "
+                                               "graph launch per search)",
                "gteps": round(m / (bfs_ms / 1e3) / 1e9, 2), "steps_per_search":
                    round(steps_total / max(1, len(picked)), 1), "sources": picked}
         eng.set_stream(None)

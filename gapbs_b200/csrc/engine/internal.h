@@ -178,9 +178,13 @@ void FreeCcScratch(CcScratch *c);
 struct BfsScratch {
   int32_t *parent = nullptr, *queue[2] = {nullptr, nullptr};
   unsigned *bm[2] = {nullptr, nullptr};
-  int64_t *deg = nullptr, *eoff = nullptr;
-  void *cnt = nullptr, *tmp = nullptr;
-  int64_t cap_n = 0, cap_tmp = 0;
+  int64_t *deg = nullptr, *eoff = nullptr, *sums = nullptr;
+  void *ctl = nullptr;  // the search's control block (bfs.cu)
+  int64_t cap_n = 0;
+  // the search loop graph and the launch plan it was captured with
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t cap_stream = nullptr;
+  std::vector<unsigned char> plan;
 };
 struct BfsStep {
   const char *kind;  // "i", "td", "e", "bu", "c" as the reference logs them
@@ -189,10 +193,12 @@ struct BfsStep {
 };
 void FreeBfsScratch(BfsScratch *b);
 // parent_old[v] (device, n entries, original ids): v's BFS parent from
-// source_old, the source itself for the source, -1 when unreached.
+// source_old, the source itself for the source, -1 when unreached.  steps
+// (nullable): the first steps with device-measured durations; *nsteps
+// (nullable): the number of steps, init included.
 cudaError_t BreadthFirstSearch(const DeviceGraph &g, BfsScratch &b, cudaStream_t s,
                                int source_old, int alpha, int beta, int32_t *parent_old,
-                               std::vector<BfsStep> *steps, std::string *err);
+                               std::vector<BfsStep> *steps, int64_t *nsteps, std::string *err);
 cudaError_t ConnectedComponents(const DeviceGraph &g, CcScratch &cs, cudaStream_t s,
                                 int32_t *out_old, std::string *err);
 // int64 CSR offsets -> int32, setting *bad for values outside [0, 2^31).

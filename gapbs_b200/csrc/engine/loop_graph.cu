@@ -8,22 +8,12 @@ namespace prgpu {
 
 namespace {
 
-// Profilers that replay kernels one by one cannot replay kernel nodes inside
-// a graph with conditional nodes.  GAPBS_PR_PLAIN_LAUNCH=1 makes Launch issue
-// the same kernels as ordinary launches instead: max_iters sweep launches
-// (those after the loop stopped return at once) each followed by a
-// one-thread kernel that advances the sweep index like the decide kernel:
-// it counts every sweep that ran, including the one that set `done`, none
-// after it, and stops the loop once the sweep index reaches max_iters.
-// Results and sweep counts are identical.
-bool PlainLaunchMode() {
-  static const bool plain = [] {
-    const char *v = std::getenv("GAPBS_PR_PLAIN_LAUNCH");
-    return v && v[0] == '1';
-  }();
-  return plain;
-}
-
+// In plain-launch mode Launch issues max_iters sweep launches (those after
+// the loop stopped return at once), each followed by a one-thread kernel
+// that advances the sweep index like the decide kernel: it counts every
+// sweep that ran, including the one that set `done`, none after it, and
+// stops the loop once the sweep index reaches max_iters.  Results and sweep
+// counts are identical.
 __global__ void loop_advance_kernel(LoopCtl *ctl, int max_iters) {
   if (threadIdx.x != 0 || blockIdx.x != 0 || ctl->halted) return;
   const int loops = ctl->loops + 1;
@@ -45,6 +35,16 @@ __global__ void loop_decide_kernel(LoopCtl *ctl, int max_iters,
 }
 
 }  // namespace
+
+// Profilers that replay kernels one by one cannot replay kernel nodes inside
+// a graph with conditional nodes.
+bool PlainLaunchMode() {
+  static const bool plain = [] {
+    const char *v = std::getenv("GAPBS_PR_PLAIN_LAUNCH");
+    return v && v[0] == '1';
+  }();
+  return plain;
+}
 
 void LoopGraph::Reset() {
   if (exec_) cudaGraphExecDestroy(exec_);

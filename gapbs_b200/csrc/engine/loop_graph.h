@@ -25,6 +25,11 @@ struct LoopCtl {
   int halted;  // plain-launch mode: the sweep that set `done` has been counted
 };
 
+// GAPBS_PR_PLAIN_LAUNCH=1: device-driven loops are issued as ordinary
+// launches instead (for profilers that cannot replay kernel nodes inside
+// graphs with conditional nodes); results are identical.
+bool PlainLaunchMode();
+
 class LoopGraph {
  public:
   LoopGraph() = default;

@@ -704,8 +704,10 @@ int pr_gpu_bfs_device(pr_gpu_t *h, int64_t source, int32_t *parent_out_dev,
   PR_CHECK(h, cudaSetDevice(h->device));
   std::string msg;
   std::vector<prgpu::BfsStep> log;
+  int64_t total = 0;
   cudaError_t e = prgpu::BreadthFirstSearch(h->g, h->bfs, h->stream, static_cast<int>(source), 15,
-                                            18, parent_out_dev, &log, &msg);
+                                            18, parent_out_dev, steps ? &log : nullptr, &total,
+                                            &msg);
   if (e != cudaSuccess)
     return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
   int k = 0;
@@ -717,7 +719,7 @@ int pr_gpu_bfs_device(pr_gpu_t *h, int64_t source, int32_t *parent_out_dev,
     steps[k].seconds = st.seconds;
     k++;
   }
-  if (nsteps) *nsteps = static_cast<int>(log.size());
+  if (nsteps) *nsteps = static_cast<int>(total);
   return PR_GPU_OK;
 }
 

@@ -137,3 +137,43 @@ def test_directed_source_without_in_edges(engine):
     check(g, 0, parent)
     kinds = [k for k, _, _ in steps]
     assert kinds[1] == "e" and kinds.count("bu") >= 3
+
+
+def test_host_stepped_mode_matches(tmp_path):
+    # GAPBS_PR_PLAIN_LAUNCH=1 runs the same step kernels launched one by one
+    # from the host (the mode profilers use); same trees, same step sequence
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    import subprocess
+    import sys
+    script = tmp_path / "plain_bfs.py"
+    script.write_text(
+        "import json, sys\n"
+        "import numpy as np\n"
+        "sys.path[:0] = [%r, %r]\n"
+        "import oracle\n"
+        "from gapbs_b200 import PageRankEngine\n"
+        "from gapbs_b200.graph import make_graph\n"
+        "from helpers import depths_from_parents\n"
+        "eng = PageRankEngine(0)\n"
+        "out = []\n"
+        "for args in ('-g 14', '-u 12', '-g 12 -k 2'):\n"
+        "    g = make_graph(args)\n"
+        "    eng.upload(g)\n"
+        "    cand = np.nonzero(np.diff(g.out_offsets) > 0)[0]\n"
+        "    for src in (int(cand[0]), int(cand[-1])):\n"
+        "        parent, steps = eng.bfs(src, with_steps=True)\n"
+        "        ok = oracle.bfs_verify(g, src, parent) and np.array_equal(\n"
+        "            depths_from_parents(parent, src), oracle.bfs_depths(g, src))\n"
+        "        out.append([args, src, bool(ok), [k for k, _, _ in steps]])\n"
+        "print(json.dumps(out))\n" % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                      os.path.dirname(os.path.abspath(__file__))))
+    res = {}
+    for mode in ("0", "1"):
+        env = dict(os.environ, GAPBS_PR_PLAIN_LAUNCH=mode)
+        r = subprocess.run([sys.executable, str(script)], env=env, capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        res[mode] = json.loads(r.stdout.strip().splitlines()[-1])
+    assert all(ok for _, _, ok, _ in res["0"]) and all(ok for _, _, ok, _ in res["1"])
+    assert [k for *_, k in res["0"]] == [k for *_, k in res["1"]]
