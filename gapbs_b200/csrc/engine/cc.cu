@@ -68,13 +68,17 @@ __device__ __forceinline__ int ld_comp_cached(const int *comp, int x) {
 __device__ void cc_link(int u, int v, int *comp, int *err) {
   int p1 = ld_comp(comp, u);
   int p2 = ld_comp_cached(comp, v);
+  // comp[u] == u read fresh: u is a root, so the first pass needs no re-read
+  // of its line when u is the higher root (most links of the first round)
+  bool u_root = p1 == u;
   for (int it = 0; p1 != p2; it++) {
     if (it >= kChaseLimit) {
       atomicExch(err, 1);
       return;
     }
     const int high = max(p1, p2), low = min(p1, p2);
-    int p_high = ld_comp_cached(comp, high);
+    int p_high = (u_root && high == u) ? u : ld_comp_cached(comp, high);
+    u_root = false;
     if (p_high == high) {
       p_high = ld_comp(comp, high);
       if (p_high == high) {
@@ -166,19 +170,31 @@ __global__ void cc_finish_thread_kernel(int32_t row0, int32_t row1,
   }
 }
 
-// Smallest original id of every component, kept at its root.  Members of
-// the component of row 0 (the largest one; half the graph on Kronecker
-// inputs) are reduced per thread and per block first, so its root takes one
-// atomic per block instead of one per vertex.
-__global__ void __launch_bounds__(256) cc_root_min_kernel(int32_t n, const int *comp,
-                                                          const int32_t *__restrict__ perm,
-                                                          int *root_min) {
+// The last compress, fused with the ids mapped back: every vertex chases
+// to its root (as cc_compress_kernel) and offers its original id to the
+// root's minimum.  Members of the component of row 0 (the largest one; half
+// the graph on Kronecker inputs) are reduced per thread and per block first,
+// so its root takes one atomic per block instead of one per vertex.
+__global__ void __launch_bounds__(256) cc_compress_min_kernel(int32_t n, int *comp,
+                                                              const int32_t *__restrict__ perm,
+                                                              int *root_min, int *err) {
   __shared__ int s_min[8];
   const int giant = 0;  // row 0 is the root of its component
   int local = INT_MAX;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride) {
-    const int c = comp[v];
+    int it = 0;
+    int c = ld_comp(comp, static_cast<int>(v));
+    int cc = ld_comp_cached(comp, c);
+    while (c != cc) {
+      if (++it >= kChaseLimit) {
+        atomicExch(err, 1);
+        break;
+      }
+      comp[v] = cc;
+      c = cc;
+      cc = ld_comp_cached(comp, c);
+    }
     if (c == giant) local = min(local, perm[v]);
     else atomicMin(root_min + c, perm[v]);
   }
@@ -276,9 +292,8 @@ cudaError_t ConnectedComponents(const DeviceGraph &g, CcScratch &cs, cudaStream_
       cc_finish_thread_kernel<<<CcGrid(active - long_rows), 256, 0, s>>>(
           long_rows, active, ooff, onbr, ioff, inbr, kRounds, giant, comp, derr);
     // roots of the rows [0, active) are rows of [0, active)
-    cc_compress_kernel<<<CcGrid(active), 256, 0, s>>>(active, comp, derr);
     fill_kernel<<<CcGrid(active), 256, 0, s>>>(active, INT_MAX, root_min);
-    cc_root_min_kernel<<<CcGrid(active), 256, 0, s>>>(active, comp, g.perm, root_min);
+    cc_compress_min_kernel<<<CcGrid(active), 256, 0, s>>>(active, comp, g.perm, root_min, derr);
     cc_label_kernel<<<grid, 256, 0, s>>>(n, active, comp, g.inv, root_min, out_old);
     e = cudaGetLastError();
   }
