@@ -715,6 +715,7 @@ def run_reference(a, dist: Dist):
                 per.append((time.perf_counter() - t0, k))
         sec = sum(p[0] for p in per)
         val = m * sum(p[1] for p in per) / sec / 1e9
+        ms_step = sec * 1e3 / a.steps
         kind, sample, cores_used = "port", "2 sweeps per step, FP32 restatement, one thread", 1
     else:
         rg, _ = capture_fd1(oracle.RefGraph.build, a.graph)
@@ -725,6 +726,7 @@ def run_reference(a, dist: Dist):
             rg.time_pagerank_pull(trials=1, max_iters=a.max_iters, epsilon=a.epsilon)
         tot, per = rg.time_pagerank_pull(trials=a.steps, max_iters=a.max_iters, epsilon=a.epsilon)
         val = m * sweeps * a.steps / tot / 1e9
+        ms_step = tot * 1e3 / a.steps
         kind, cores_used = "reference", cores
         sample = (f"each step one full PageRankPull solve ({sweeps} sweeps) of {a.graph.strip()} "
                   f"by the reference compiled from source, OpenMP on {cores} threads")
@@ -736,6 +738,7 @@ def run_reference(a, dist: Dist):
         "n_gpus": dist.world,
         "steps": a.steps,
         "warmup": a.warmup,
+        "ms_per_step": round(ms_step, 4),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
