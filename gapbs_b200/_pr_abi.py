@@ -21,7 +21,7 @@ SYMBOLS = (
     "pr_gpu_connected_components_device",
     "pr_gpu_adjoint", "pr_gpu_adjoint_device", "pr_gpu_set_stream",
     "pr_gpu_set_batch_tile", "pr_gpu_get_batch_tile", "pr_gpu_last_timing",
-    "pr_gpu_graph_info", "pr_gpu_measure_gather_rate", "pr_gpu_run_noalloc", "pr_gpu_destroy", "pr_gpu_last_error",
+    "pr_gpu_graph_info", "pr_gpu_measure_gather_rate", "pr_gpu_measure_row_gather_rate", "pr_gpu_run_noalloc", "pr_gpu_destroy", "pr_gpu_last_error",
 )
 
 
@@ -65,6 +65,8 @@ def declare(lib):
     lib.pr_gpu_graph_info.restype = c_int
     lib.pr_gpu_measure_gather_rate.argtypes = [c_int, c_int64, POINTER(c_double)]
     lib.pr_gpu_measure_gather_rate.restype = c_int
+    lib.pr_gpu_measure_row_gather_rate.argtypes = [c_int, c_int64, c_int, POINTER(c_double)]
+    lib.pr_gpu_measure_row_gather_rate.restype = c_int
     lib.pr_gpu_run_noalloc.argtypes = [c_int, c_int64, c_int64, P, P, P, c_int, c_double, c_float,
                                        P, P, P, P, c_char_p, c_size_t]
     lib.pr_gpu_run_noalloc.restype = c_int

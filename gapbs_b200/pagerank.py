@@ -321,6 +321,19 @@ def measure_gather_rate(array_bytes: int, device: int = 0) -> float:
     return out.value
 
 
+def measure_row_gather_rate(array_bytes: int, row_bytes: int, device: int = 0) -> float:
+    """Bytes per second gathered as random rows of row_bytes with 16-byte
+    loads (see pr_gpu_measure_row_gather_rate): the ceiling of a batched
+    sweep's contrib-row gathers when the tile fits in L2."""
+    lib = pr_lib()
+    out = c_double()
+    rc = lib.pr_gpu_measure_row_gather_rate(int(device), int(array_bytes), int(row_bytes),
+                                            byref(out))
+    if rc != 0:
+        raise PageRankError(rc, "pr_gpu_measure_row_gather_rate failed")
+    return out.value
+
+
 def print_step(step: int, value: float) -> None:
     """The reference's -l line (src/util.h:37-46): '%5s%23.5lf'."""
     print(f"{step:>5d}{value:23.5f}")

@@ -210,6 +210,14 @@ int pr_gpu_graph_info(const pr_gpu_t *h, int64_t *n, int64_t *m,
  * the reference. */
 int pr_gpu_measure_gather_rate(int device, int64_t array_bytes, double *gathers_per_s);
 
+/* The same for whole rows: gathers random rows of row_bytes (16..512, a power
+ * of two) from an array of about array_bytes with 16-byte loads, row_bytes/16
+ * lanes per row, and returns the bytes gathered per second.  A batched PPR
+ * sweep gathers one row of its contrib tile (4 bytes per column) per edge,
+ * so this is its gather roofline.  No counterpart in the reference. */
+int pr_gpu_measure_row_gather_rate(int device, int64_t array_bytes, int row_bytes,
+                                   double *bytes_per_s);
+
 /* Upper limits of pr_gpu_run_noalloc (sizes of its fixed scratch area). */
 #define PR_GPU_NOALLOC_MAX_VERTICES (1 << 20)
 #define PR_GPU_NOALLOC_MAX_ITERS 1024
