@@ -51,3 +51,18 @@ def test_engine_library_is_sm100a():
     """The engine is compiled for sm_100a only (no other targets)."""
     mk = open(os.path.join(ROOT, "Makefile")).read()
     assert "arch=compute_100a,code=sm_100a" in mk
+
+
+def test_gather_probes_reject_bad_arguments():
+    """The roofline probes check their arguments before touching a device."""
+    lib = ctypes.CDLL(HEADERS["pr_gpu.h"])
+    out = ctypes.c_double()
+    lib.pr_gpu_measure_gather_rate.argtypes = [ctypes.c_int, ctypes.c_int64,
+                                               ctypes.POINTER(ctypes.c_double)]
+    lib.pr_gpu_measure_row_gather_rate.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int,
+                                                   ctypes.POINTER(ctypes.c_double)]
+    assert lib.pr_gpu_measure_gather_rate(0, 1024, ctypes.byref(out)) == -1
+    assert lib.pr_gpu_measure_gather_rate(0, 1 << 20, None) == -1
+    for row_bytes in (0, 8, 24, 1024):
+        assert lib.pr_gpu_measure_row_gather_rate(0, 1 << 20, row_bytes, ctypes.byref(out)) == -1
+    assert lib.pr_gpu_measure_row_gather_rate(0, 1 << 20, 256, None) == -1

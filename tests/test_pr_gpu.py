@@ -155,3 +155,13 @@ def test_bins_cover_all_rows(engine):
     info = engine.graph_info()
     assert sum(info["bin_rows"]) == g.num_nodes
     assert info["max_degree"] == int(np.diff(g.in_offsets).max())
+
+
+def test_gather_roofline_probes(engine):
+    # the ceilings bench.py divides by: positive and of the right order
+    from gapbs_b200.pagerank import measure_gather_rate, measure_row_gather_rate
+    g4 = measure_gather_rate(64 << 20, 0)
+    assert 1e10 < g4 < 1e13  # 4-byte loads per second
+    rows = [measure_row_gather_rate(64 << 20, rb, 0) for rb in (16, 256)]
+    assert all(1e11 < r < 1e14 for r in rows)  # bytes per second
+    assert rows[1] > rows[0]  # whole rows move more bytes per request
