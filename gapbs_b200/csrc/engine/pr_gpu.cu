@@ -7,6 +7,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -94,9 +95,17 @@ class CopyPool {
   }
 
  private:
-  CopyPool()
-      : nt_(static_cast<int>(std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2)))) {
+  CopyPool() : nt_(Threads()) {
     for (int t = 1; t < nt_; t++) std::thread([this, t] { Worker(t); }).detach();
+  }
+
+  // half the hardware threads, at most 8 (GAPBS_PR_COPY_THREADS overrides;
+  // on a 16-core host 16 or 24 threads staged a 4.3 GB CSR more slowly than
+  // 8: the copy is bound by host memory bandwidth)
+  static int Threads() {
+    const char *v = std::getenv("GAPBS_PR_COPY_THREADS");
+    if (v && *v) return static_cast<int>(std::max(1L, std::min(64L, std::strtol(v, nullptr, 10))));
+    return static_cast<int>(std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2)));
   }
 
   void Share(int t) const {
