@@ -587,10 +587,12 @@ def run_ppr(a, dev):
     steps = float(bsweeps.max())
     gathered = 4.0 * m * col_sweeps
     streamed = steps * (4.0 * m + 4.0 * (n + 1)) + 12.0 * n * col_sweeps
-    # the ceiling of those gathers: random 256-byte rows (a 64-column tile
-    # row) with 16-byte loads from an L2-resident array, measured now
+    # the ceilings of those gathers: random 256-byte rows (a 64-column tile
+    # row) with 16-byte loads from an L2-resident array and from a 1 GB one
+    # (the g22 tile's size, served by HBM), measured now
     from gapbs_b200.pagerank import measure_row_gather_rate
     row_peak = measure_row_gather_rate(64 << 20, 4 * 64, dev) / 1e9
+    row_peak_hbm = measure_row_gather_rate(1 << 30, 4 * 64, dev) / 1e9
     gathered_gbs = gathered / (b_ms / 1e3) / 1e9
     return {
         "workload": f"{a.ppr_cols} PPR vectors on {a.ppr_graph.strip()} (N={n}, M={m}), seed sets "
@@ -602,7 +604,9 @@ def run_ppr(a, dev):
             "gather": {"achieved": round(gathered_gbs, 1), "peak": round(row_peak, 1),
                        "unit": "GB/s", "frac": round(gathered_gbs / row_peak, 4),
                        "peak_source": "measured in this run: random 256-byte rows (16-byte "
-                                      "loads) from a 64 MB L2-resident array"},
+                                      "loads) from a 64 MB L2-resident array",
+                       "peak_1gb_array": round(row_peak_hbm, 1),
+                       "frac_1gb_array": round(gathered_gbs / row_peak_hbm, 4)},
             "note": "gathered bytes come mostly from L2 (78 % hit, profiles/"
                     "batch_sweep_g20_full.md); the sweep is bound by gather latency",
         },
