@@ -607,8 +607,9 @@ def run_ppr(a, dev):
                                       "loads) from a 64 MB L2-resident array",
                        "peak_1gb_array": round(row_peak_hbm, 1),
                        "frac_1gb_array": round(gathered_gbs / row_peak_hbm, 4)},
-            "note": "gathered bytes come mostly from L2 (78 % hit, profiles/"
-                    "batch_sweep_g20_full.md); the sweep is bound by gather latency",
+            "note": "hub rows hit L2, the rest come from HBM (63 % L2 hit at g22, profiles/"
+                    "batch_sweep_g22_metrics.md): the rate lies between the L2-resident "
+                    "and the 1 GB-array row-gather ceilings",
         },
         "batched_gteps": round(b_gteps, 3),
         "batched_ms": round(b_ms, 3),
