@@ -102,7 +102,9 @@ int pr_gpu_download_csr(pr_gpu_t *h, int64_t *out_off, int32_t *out_nbr);
 /* One step of a breadth-first search as the reference logs it with -l
  * (src/bfs.cc:118-160): kind "i" (init), "td" (top-down; count = next
  * frontier size), "e" (queue to bitmap), "bu" (bottom-up; count = vertices
- * found), "c" (bitmap to queue); count -1 where the reference prints none. */
+ * found), "c" (bitmap to queue); count -1 where the reference prints none.
+ * seconds: the step's duration measured on the device (the steps run as
+ * one CUDA graph, so no host clock sees them one by one). */
 typedef struct pr_gpu_bfs_step {
   char kind[4];
   int64_t count;
