@@ -177,3 +177,26 @@ def test_host_stepped_mode_matches(tmp_path):
         res[mode] = json.loads(r.stdout.strip().splitlines()[-1])
     assert all(ok for _, _, ok, _ in res["0"]) and all(ok for _, _, ok, _ in res["1"])
     assert [k for *_, k in res["0"]] == [k for *_, k in res["1"]]
+
+
+def test_step_log_truncated_to_caller_buffer(engine):
+    # pr_gpu_bfs fills at most max_steps records and reports the full count
+    import ctypes
+    g = make_graph("-g 14")
+    engine.upload(g)
+    src = int(np.argmax(np.diff(g.out_offsets)))
+    full_parent, full = engine.bfs(src, with_steps=True)
+    lib = engine._lib
+    parent = np.empty(g.num_nodes, np.int32)
+    rec = np.zeros(2, dtype=np.dtype([("kind", "S4"), ("count", "<i8"), ("seconds", "<f8")],
+                                      align=True))
+    nsteps = ctypes.c_int()
+    rc = lib.pr_gpu_bfs(engine._h, src, parent.ctypes.data, rec.ctypes.data, 2,
+                        ctypes.byref(nsteps))
+    assert rc == 0
+    assert nsteps.value == len(full) > 2
+    assert [r["kind"].decode() for r in rec] == [k for k, _, _ in full[:2]]
+    assert oracle.bfs_verify(g, src, parent)
+    # no step buffer at all: still the count
+    rc = lib.pr_gpu_bfs(engine._h, src, parent.ctypes.data, None, 0, ctypes.byref(nsteps))
+    assert rc == 0 and nsteps.value == len(full)
