@@ -39,7 +39,8 @@ int gapbs_graph_from_edges(gapbs_graph_t **out, const int32_t *u,
 
 /* An undirected graph of n vertices and m CSR entries whose arrays the
  * caller fills (for example from pr_gpu_download_csr): *off receives the
- * n + 1 offsets, *nbr the m neighbours, both owned by the graph. */
+ * n + 1 offsets, *nbr the m neighbours, both owned by the graph (the
+ * reference's CSRGraph(num_nodes, index, neighs), src/graph.h:138-143). */
 int gapbs_graph_new_undirected(gapbs_graph_t **out, int64_t n, int64_t m,
                                int64_t **off, int32_t **nbr);
 
@@ -51,16 +52,21 @@ int gapbs_rmat_permutation(int scale, int32_t *perm);
 /* Writes the .sg serialized layout (src/writer.h:39-69). */
 int gapbs_graph_write_sg(const gapbs_graph_t *g, const char *path);
 
+/* ~CSRGraph (src/graph.h:165-167). */
 void gapbs_graph_free(gapbs_graph_t *g);
 
+/* CSRGraph::num_nodes / num_edges / num_edges_directed / directed
+ * (src/graph.h:189-203); undirected graphs count each edge once in
+ * num_edges. */
 int64_t gapbs_graph_num_nodes(const gapbs_graph_t *g);
-/* Undirected graphs count each edge once (src/graph.h:193-203). */
 int64_t gapbs_graph_num_edges(const gapbs_graph_t *g);
 int64_t gapbs_graph_num_edges_directed(const gapbs_graph_t *g);
 int gapbs_graph_directed(const gapbs_graph_t *g);
 
-/* CSR views owned by the graph (valid until gapbs_graph_free).  For an
- * undirected graph the in-views return the out-arrays. */
+/* CSR views owned by the graph (valid until gapbs_graph_free): the arrays
+ * behind CSRGraph::out_neigh / in_neigh (src/graph.h:214-222) and
+ * VertexOffsets (src/graph.h:251-259), offsets as int64 counts.  For an undirected graph the in-views
+ * return the out-arrays. */
 const int64_t *gapbs_graph_out_offsets(const gapbs_graph_t *g);
 const int32_t *gapbs_graph_out_neighbors(const gapbs_graph_t *g);
 const int64_t *gapbs_graph_in_offsets(const gapbs_graph_t *g);

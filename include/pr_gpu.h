@@ -45,7 +45,9 @@ extern "C" {
 
 typedef struct pr_gpu pr_gpu_t;
 
-/* Creates a handle bound to CUDA device `device` with its own stream. */
+/* Creates a handle bound to CUDA device `device` with its own stream.  The
+ * handle owns the device mirror of one CSRGraph (src/graph.h:98-273, which
+ * the reference keeps in host memory only) and every device allocation. */
 int pr_gpu_create(pr_gpu_t **h, int device);
 
 /* Uploads a CSR graph and builds the device mirror (degree-ordered rows and
@@ -96,7 +98,9 @@ int pr_gpu_generate(pr_gpu_t *h, int uniform, int scale, int degree,
                     const int32_t *perm, int64_t *n_out, int64_t *m_out);
 
 /* Copies the CSR of the last pr_gpu_generate to host buffers (n_out + 1
- * offsets, m_out neighbours), then frees the device copy. */
+ * offsets, m_out neighbours), then frees the device copy: the host CSR the
+ * reference's BuilderBase::MakeGraph returns (src/builder.h:343-364), for
+ * host code such as PRVerifier. */
 int pr_gpu_download_csr(pr_gpu_t *h, int64_t *out_off, int32_t *out_nbr);
 
 /* One step of a breadth-first search as the reference logs it with -l
@@ -151,8 +155,9 @@ int pr_gpu_run(pr_gpu_t *h, int max_iters, double epsilon, float damping,
                int ncols, const float *teleport, float *scores_out,
                int32_t *sweeps_out, double *err_trace);
 
-/* Same as pr_gpu_run with teleport / scores_out as DEVICE pointers on the
- * handle's GPU (no host copies; the call still returns after the solve). */
+/* Same as pr_gpu_run (PageRankPull, src/pr_spmv.cc:35-61) with teleport /
+ * scores_out as DEVICE pointers on the handle's GPU (no host copies; the
+ * call still returns after the solve). */
 int pr_gpu_run_device(pr_gpu_t *h, int max_iters, double epsilon,
                       float damping, int ncols, const float *teleport_dev,
                       float *scores_out_dev, int32_t *sweeps_out,
@@ -172,13 +177,15 @@ int pr_gpu_adjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping,
                    float *grad_teleport, float *grad_edge_w,
                    int32_t *sweeps_out);
 
-/* Device-pointer form of pr_gpu_adjoint. */
+/* Device-pointer form of pr_gpu_adjoint (no counterpart in the reference). */
 int pr_gpu_adjoint_device(pr_gpu_t *h, int max_iters, double epsilon,
                           float damping, const float *loss_w_dev,
                           const float *scores_dev, float *grad_teleport_dev,
                           float *grad_edge_w_dev, int32_t *sweeps_out);
 
-/* Column tile width of batched (ncols > 1) solves: 8, 16, 32 or 64 score
+/* Engine controls below have no counterpart in the reference.
+ *
+ * Column tile width of batched (ncols > 1) solves: 8, 16, 32 or 64 score
  * columns per block row, or 0 (the default) to let the engine's autotuner
  * time each width on the first batched solve of a graph and column count
  * and keep the fastest.  pr_gpu_get_batch_tile reports the width in use
@@ -197,8 +204,9 @@ int pr_gpu_set_stream(pr_gpu_t *h, void *stream);
 int pr_gpu_last_timing(const pr_gpu_t *h, double *sweep_ms, double *total_ms,
                        int64_t *kernel_launches);
 
-/* Graph facts after upload: vertices, entries, rows per vertex bin
- * (nbins entries, bin order as documented in the engine), max in-degree. */
+/* Graph facts after upload: vertices and entries (CSRGraph::num_nodes,
+ * num_edges_directed, src/graph.h:193-203), rows per vertex bin (nbins
+ * entries, bin order as documented in the engine), max in-degree. */
 int pr_gpu_graph_info(const pr_gpu_t *h, int64_t *n, int64_t *m,
                       int64_t *max_degree, int64_t *bin_rows, int nbins);
 
@@ -259,6 +267,8 @@ int pr_gpu_run_noalloc(int device, int64_t n, int64_t m,
                        int32_t *sweeps_out, double *err_trace, void *stream,
                        char *err_msg, size_t err_len);
 
+/* Frees the handle and all its device memory (the mirror's counterpart of
+ * ~CSRGraph, src/graph.h:165-167).  NULL is ignored. */
 void pr_gpu_destroy(pr_gpu_t *h);
 
 /* Message for the last failure on h (h may be NULL for create failures). */
