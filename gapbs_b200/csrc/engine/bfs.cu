@@ -466,9 +466,13 @@ __device__ __forceinline__ bool in_front(const unsigned *__restrict__ front, int
   return (__ldg(front + (u >> 5)) >> (u & 31)) & 1u;
 }
 
-// Bottom-up step: each warp owns 32 consecutive vertices (one bitmap word).
-// Only rows [0, rows) have in-neighbours (rows are sorted by in-degree), so
-// only their words are visited; the words after them stay zero.
+// Bottom-up step: each warp owns two bitmap words (32 consecutive vertices
+// each) at a time and every lane walks its two vertices' in-lists together,
+// so two independent load chains (neighbour id, then its frontier bit) are
+// in flight per lane; each vertex still takes the first in-neighbour in list
+// order found in the frontier.  Only rows [0, rows) have in-neighbours (rows
+// are sorted by in-degree), so only their words are visited; the words after
+// them stay zero.
 __global__ void bfs_bu_kernel(BfsCtl *ctl, int32_t rows, const int32_t *__restrict__ ioff,
                               const int32_t *__restrict__ inbr, const unsigned *bm0,
                               const unsigned *bm1, unsigned *nbm0, unsigned *nbm1,
@@ -482,22 +486,46 @@ __global__ void bfs_bu_kernel(BfsCtl *ctl, int32_t rows, const int32_t *__restri
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
   unsigned long long awake = 0;
   for (int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; w < words;
-       w += warps) {
-    const int64_t v = (w << 5) + lane;
-    bool found = false;
-    if (v < n && parent[v] < 0) {
-      for (int j = ioff[v]; j < ioff[v + 1]; j++) {
-        const int u = inbr[j];
-        if (in_front(front, u)) {
-          parent[v] = __ldg(perm + u);
-          found = true;
-          break;
-        }
+       w += 2 * warps) {
+    const int64_t w2 = w + warps;  // the warp's second word (warp-uniform test)
+    const int64_t v1 = (w << 5) + lane, v2 = (w2 << 5) + lane;
+    int j1 = 0, e1 = 0, j2 = 0, e2 = 0;
+    if (v1 < n && parent[v1] < 0) {
+      j1 = ioff[v1];
+      e1 = ioff[v1 + 1];
+    }
+    if (w2 < words && v2 < n && parent[v2] < 0) {
+      j2 = ioff[v2];
+      e2 = ioff[v2 + 1];
+    }
+    int p1 = -1, p2 = -1;  // the in-neighbour found (mirror row), if any
+    while (j1 < e1 || j2 < e2) {
+      const int u1 = j1 < e1 ? inbr[j1] : -1;
+      const int u2 = j2 < e2 ? inbr[j2] : -1;
+      const bool h1 = u1 >= 0 && in_front(front, u1);
+      const bool h2 = u2 >= 0 && in_front(front, u2);
+      if (h1) {
+        p1 = u1;
+        e1 = j1;  // chain 1 done
+      } else {
+        j1++;
+      }
+      if (h2) {
+        p2 = u2;
+        e2 = j2;
+      } else {
+        j2++;
       }
     }
-    const unsigned word = __ballot_sync(0xffffffffu, found);
-    if (lane == 0) next[w] = word;
-    awake += found ? 1 : 0;
+    if (p1 >= 0) parent[v1] = __ldg(perm + p1);
+    if (p2 >= 0) parent[v2] = __ldg(perm + p2);
+    const unsigned word1 = __ballot_sync(0xffffffffu, p1 >= 0);
+    if (lane == 0) next[w] = word1;
+    if (w2 < words) {
+      const unsigned word2 = __ballot_sync(0xffffffffu, p2 >= 0);
+      if (lane == 0) next[w2] = word2;
+    }
+    awake += (p1 >= 0 ? 1 : 0) + (p2 >= 0 ? 1 : 0);
   }
   for (int o = 16; o > 0; o >>= 1) awake += __shfl_xor_sync(0xffffffffu, awake, o);
   if (lane == 0 && awake) atomicAdd(&ctl->cnt.awake, awake);
