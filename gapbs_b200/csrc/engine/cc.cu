@@ -100,13 +100,25 @@ __global__ void cc_init_kernel(int32_t n, int *comp) {
 }
 
 // One sampling round (src/cc.cc:100-106): vertex u links with its r-th
-// out-neighbour.
+// out-neighbour.  Each thread takes two vertices per pass and loads both
+// neighbour ids (random reads of the neighbour array, one HBM sector each)
+// before either link, so two such reads are in flight per thread.
 __global__ void cc_sample_kernel(int32_t n, const int32_t *__restrict__ off,
                                  const int32_t *__restrict__ nbr, int r, int *comp, int *err) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t u = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u < n; u += stride) {
-    const int s = off[u], e = off[u + 1];
-    if (s + r < e) cc_link(static_cast<int>(u), nbr[s + r], comp, err);
+  for (int64_t u = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u < n;
+       u += 2 * stride) {
+    const int64_t u2 = u + stride;
+    const int s1 = off[u], e1 = off[u + 1];
+    int s2 = 0, e2 = 0;
+    if (u2 < n) {
+      s2 = off[u2];
+      e2 = off[u2 + 1];
+    }
+    const int v1 = s1 + r < e1 ? nbr[s1 + r] : -1;
+    const int v2 = s2 + r < e2 ? nbr[s2 + r] : -1;
+    if (v1 >= 0) cc_link(static_cast<int>(u), v1, comp, err);
+    if (v2 >= 0) cc_link(static_cast<int>(u2), v2, comp, err);
   }
 }
 
