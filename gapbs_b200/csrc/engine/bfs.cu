@@ -34,8 +34,9 @@
 // Top-down work is spread over the frontier's edges, not its vertices
 // (frontier degrees are scanned, each thread takes edges and finds its
 // vertex by a forward search in the scan), so a hub in the frontier does not
-// serialise a warp.  Bottom-up work: each warp owns 32 consecutive vertices
-// and writes their bitmap word with one ballot.
+// serialise a warp.  Bottom-up work: each warp owns two words of 32
+// consecutive vertices at a time, walks the two vertices of every lane
+// together, and writes each bitmap word with one ballot.
 #include <cuda_runtime.h>
 
 #include <algorithm>
