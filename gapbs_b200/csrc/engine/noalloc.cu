@@ -7,8 +7,14 @@
 // synchronisation cudaMalloc / cudaFree can cause in the middle of serving.
 // They pass device buffers they already own (the CSR in, the scores out) and
 // this entry point uses only a fixed scratch area that lives in this file as
-// a static __device__ array, loaded with the library onto every GPU that uses
-// it and kept until the process exits.
+// a static __device__ array.  The CUDA runtime loads this file's device code
+// and that array onto a GPU lazily, at the first call on that GPU (the
+// cudaGetSymbolAddress in ScratchFor): that one load reserves about 8.4 MB of
+// device memory plus the module's code, and the GPU keeps it until the
+// process exits.  Callers whose pool allocator reserves the GPU's memory
+// must therefore make their first call on each device (max_iters = 0 on any
+// small graph is enough) before the pool takes its memory, and before any
+// stream capture; later calls load nothing and allocate nothing.
 //
 // Limits: at most kNoAllocMaxVertices vertices and kNoAllocMaxIters sweeps;
 // larger requests are rejected.  All calls share the one scratch array, so
@@ -138,7 +144,7 @@ noalloc_sweep_kernel(unsigned char *scratch, int32_t n, const int32_t *__restric
   __shared__ int s_last;
   const int lane = threadIdx.x & 31;
   const int warps = gridDim.x * (kNoAllocThreads / 32);
-  float err = 0.f;
+  double err = 0.0;  // each |new - old| added in FP64, as src/pr_spmv.cc:53 does
   for (int u = blockIdx.x * (kNoAllocThreads / 32) + (threadIdx.x >> 5); u < n; u += warps) {
     const int rs = in_off[u], re = in_off[u + 1];
     float acc = 0.f;
@@ -149,10 +155,10 @@ noalloc_sweep_kernel(unsigned char *scratch, int32_t n, const int32_t *__restric
       const float nw = __fadd_rn(base, __fmul_rn(damping, acc));
       score[u] = nw;
       cout[u] = __fdiv_rn(nw, noalloc_degree(in_off, out_deg, u));
-      err += fabsf(__fsub_rn(nw, old));
+      err += static_cast<double>(fabsf(__fsub_rn(nw, old)));
     }
   }
-  const double block_err = block_sum_d<kNoAllocThreads>(static_cast<double>(err), sred);
+  const double block_err = block_sum_d<kNoAllocThreads>(err, sred);
   if (threadIdx.x == 0) {
     s.partial[blockIdx.x] = block_err;
     __threadfence();
@@ -176,8 +182,12 @@ noalloc_sweep_kernel(unsigned char *scratch, int32_t n, const int32_t *__restric
 }
 
 // Device address of the scratch array, taken once per device by the first
-// call on that device (with that device current).  That first call should be
-// made before any stream capture begins.
+// call on that device (with that device current); taking it loads the
+// module onto that device.  The address is cached per device index, so it
+// belongs to the device's primary context (the one the runtime API uses);
+// a caller that switches the device to another driver-API context gets the
+// primary context's array.  That first call should be made before any stream
+// capture begins.
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 void *g_scratch_ptr[kMaxDevices] = {};

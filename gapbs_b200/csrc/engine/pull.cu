@@ -19,8 +19,9 @@
 //         lane reads whole aligned 4-entry chunks and masks entries outside
 //         its row), two chunks in flight per lane, xor-tree group sum;
 //   ZERO  rows without in-neighbours: new = base.
-// The L1 error is reduced in FP64 with a deterministic two-stage tree
-// (per-block partials -> per-512-block group -> total).
+// Every |new - old| is added to an FP64 per-thread sum (the reference adds
+// each to a double, src/pr_spmv.cc:42,53), then reduced with a deterministic
+// two-stage tree (per-block partials -> per-512-block group -> total).
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -247,7 +248,7 @@ __device__ __forceinline__ float hub_segment(const PullArgs &a, const float *cin
 // One warp task of the ZERO bin: 32 * kZeroRowsPerThread rows without
 // in-neighbours (new = base).
 template <bool W, bool DIR, int KIND>
-__device__ __forceinline__ float zero_task(const PullArgs &a, float *cout, int task, int lane32,
+__device__ __forceinline__ double zero_task(const PullArgs &a, float *cout, int task, int lane32,
                                            uint64_t ps, uint64_t pl) {
   constexpr int kRows = 32 * kZeroRowsPerThread;
   const int row0 = a.bin_row[kBinZero] + task * kRows;
@@ -258,7 +259,7 @@ __device__ __forceinline__ float zero_task(const PullArgs &a, float *cout, int t
     const int u = row0 + i * 32 + lane32;
     old[i] = u < end ? ld_score(a.score + u, ps) : 0.f;
   }
-  float err = 0.f;
+  double err = 0.0;
 #pragma unroll
   for (int i = 0; i < kZeroRowsPerThread; i++) {
     const int u = row0 + i * 32 + lane32;
@@ -270,7 +271,7 @@ __device__ __forceinline__ float zero_task(const PullArgs &a, float *cout, int t
       // directed graph; its contrib is then read by the next sweep.
       if (KIND == kKindAdjoint) st_hint_f32(cout + u, nw, pl);
       else if (W || DIR) st_hint_f32(cout + u, __fdiv_rn(nw, denom_of<W, DIR>(a, u, 0, 0)), pl);
-      err += fabsf(__fsub_rn(nw, old[i]));
+      err += static_cast<double>(fabsf(__fsub_rn(nw, old[i])));
     }
   }
   return err;
@@ -293,7 +294,8 @@ pull_sweep_kernel(const PullArgs a) {
   const uint64_t ps = policy_evict_first();
   const uint64_t pg = policy_evict_last();
   const uint64_t pl = pg;
-  float err = 0.f;
+  // every |new - old| is added in FP64, as the reference adds it to a double
+  double err = 0.0;
   for (int seg = blockIdx.x; seg < a.nseg; seg += gridDim.x)
     err += hub_segment<W, DIR, KIND>(a, cin, cout, sredf, seg, ps, pg, pl);
   const int lane32 = threadIdx.x & 31;
@@ -317,7 +319,7 @@ pull_sweep_kernel(const PullArgs a) {
       default: err += zero_task<W, DIR, KIND>(a, cout, k, lane32, ps, pl); break;
     }
   }
-  const double block_err = block_sum_d<kSweepThreads>(static_cast<double>(err), sred);
+  const double block_err = block_sum_d<kSweepThreads>(err, sred);
   grid_finish(a, it, block_err, sred);
 }
 
@@ -335,7 +337,7 @@ pull_generic_kernel(const PullArgs a) {
   const uint64_t pg = policy_evict_last();
   const int lane = threadIdx.x & 31;
   const int warps = a.nblocks * (kSweepThreads / 32);
-  float err = 0.f;
+  double err = 0.0;
   for (int u = blockIdx.x * (kSweepThreads / 32) + (threadIdx.x >> 5); u < a.n; u += warps) {
     const int s = a.rowoff[u], e = a.rowoff[u + 1];
     float acc = lane_partial<32, W>(a, cin, s, e, lane, ps, pg);
@@ -343,7 +345,7 @@ pull_generic_kernel(const PullArgs a) {
     if (lane == 0)
       err += finish_row<W, false, KIND>(a, cout, u, s, e, acc, ld_score(a.score + u, ps), ps, pg);
   }
-  const double block_err = block_sum_d<kSweepThreads>(static_cast<double>(err), sred);
+  const double block_err = block_sum_d<kSweepThreads>(err, sred);
   grid_finish(a, it, block_err, sred);
 }
 

@@ -251,14 +251,20 @@ int pr_gpu_measure_row_gather_rate(int device, int64_t array_bytes, int row_byte
  * sweep < epsilon or after max_iters sweeps) up to FP32 summation order.
  *
  * Its working memory is one fixed scratch area compiled into the library
- * (about 8.4 MB, held on every GPU the library runs on until the process
- * exits), so n may be at most PR_GPU_NOALLOC_MAX_VERTICES and max_iters at
- * most PR_GPU_NOALLOC_MAX_ITERS; larger requests return PR_GPU_ERANGE with a
- * message.  The first call on a device looks up that area's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture
- * begins.  All calls share the area: calls whose GPU work overlaps in time (several
- * host threads, or several streams, on one device) race on it and must be
- * serialised by the caller.  Returns PR_GPU_OK or a PR_GPU_E* code; err_msg
+ * (about 8.4 MB), so n may be at most PR_GPU_NOALLOC_MAX_VERTICES and
+ * max_iters at most PR_GPU_NOALLOC_MAX_ITERS; larger requests return
+ * PR_GPU_ERANGE with a message.  The CUDA runtime loads that area onto a GPU
+ * at the first call on that GPU (the call looks up its device address with
+ * cudaGetSymbolAddress, which loads the library's module there): that first
+ * call reserves the area and the module's code, and the GPU holds them until
+ * the process exits.  So make the first call on each device -- max_iters = 0
+ * on any small graph you hold on the device will do -- before your pool
+ * allocator reserves the GPU's memory and before any stream capture begins;
+ * later calls allocate nothing.  The address is kept per device index and
+ * belongs to the device's primary context (the one the CUDA runtime API
+ * uses).  All calls share the area: calls whose GPU work overlaps in time
+ * (several host threads, or several streams, on one device) race on it and
+ * must be serialised by the caller.  Returns PR_GPU_OK or a PR_GPU_E* code; err_msg
  * (err_len bytes, nullable) receives a message on failure. */
 int pr_gpu_run_noalloc(int device, int64_t n, int64_t m,
                        const int32_t *in_off_dev, const int32_t *in_nbr_dev,
