@@ -13,6 +13,10 @@ PR_GPU_ENOGRAPH = -4
 PR_GPU_EGRAPH = -5
 PR_GPU_ERANGE = -6
 
+PR_GPU_SWEEP_AUTO = 0
+PR_GPU_SWEEP_GATHER = 1
+PR_GPU_SWEEP_BLOCKED = 2
+
 # Every symbol include/pr_gpu.h declares.
 SYMBOLS = (
     "pr_gpu_create", "pr_gpu_upload", "pr_gpu_upload_sg", "pr_gpu_generate", "pr_gpu_download_csr",
@@ -20,7 +24,8 @@ SYMBOLS = (
     "pr_gpu_connected_components",
     "pr_gpu_connected_components_device",
     "pr_gpu_adjoint", "pr_gpu_adjoint_device", "pr_gpu_set_stream",
-    "pr_gpu_set_batch_tile", "pr_gpu_get_batch_tile", "pr_gpu_last_timing",
+    "pr_gpu_set_batch_tile", "pr_gpu_get_batch_tile", "pr_gpu_set_sweep_layout",
+    "pr_gpu_sweep_layout_info", "pr_gpu_last_timing",
     "pr_gpu_graph_info", "pr_gpu_measure_gather_rate", "pr_gpu_measure_row_gather_rate", "pr_gpu_run_noalloc", "pr_gpu_destroy", "pr_gpu_last_error",
 )
 
@@ -56,6 +61,12 @@ def declare(lib):
     lib.pr_gpu_set_batch_tile.restype = c_int
     lib.pr_gpu_get_batch_tile.argtypes = [P, POINTER(c_int)]
     lib.pr_gpu_get_batch_tile.restype = c_int
+    lib.pr_gpu_set_sweep_layout.argtypes = [P, c_int, c_int, c_int]
+    lib.pr_gpu_set_sweep_layout.restype = c_int
+    lib.pr_gpu_sweep_layout_info.argtypes = [P, POINTER(c_int), POINTER(c_int), POINTER(c_int),
+                                             POINTER(c_int64), POINTER(c_int64), POINTER(c_int64),
+                                             POINTER(c_int)]
+    lib.pr_gpu_sweep_layout_info.restype = c_int
     lib.pr_gpu_set_stream.argtypes = [P, P]
     lib.pr_gpu_set_stream.restype = c_int
     lib.pr_gpu_last_timing.argtypes = [P, POINTER(c_double), POINTER(c_double), POINTER(c_int64)]

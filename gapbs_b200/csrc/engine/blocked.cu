@@ -1,0 +1,388 @@
+// blocked.cu -- the two kernels of a slice-blocked pull sweep (see blocked.h).
+//
+// The replaced loop is src/pr_spmv.cc:46-54: for every row u, the float sum
+// of contrib[v] over its in-neighbours, then new = base + d * sum, the FP64
+// L1 change and (src/pr_spmv.cc:43-45) the next contrib = new / out_degree.
+// Phase 1 (slice_partial_kernel) forms, per (row, source slice) pair, the
+// float sum of that slice's contribs; phase 2 (bin_row_kernel) sums each
+// row's pair partials in slice order and updates the row.  Every sum is a
+// fixed tree over a fixed layout, so two runs give identical bits.
+#include <cuda_runtime.h>
+
+#include "blocked.h"
+#include "common.cuh"
+#include "sweep_reduce.cuh"
+
+namespace prgpu {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint4 ld_stream_u4(const uint4 *p, uint64_t pol) {
+  uint4 r;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(p), "l"(pol));
+  return r;
+}
+
+// Shared-memory float at byte address base + 4 i (32-bit shared-window
+// address), so that the compiler issues a shared load with 32-bit address
+// arithmetic whatever it can prove about the pointer it came from.
+__device__ __forceinline__ float lds_f32(unsigned base, unsigned i) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(base + (i << 2)));
+  return v;
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// Asynchronous global -> shared copies (cp.async): the issuing thread does
+// not wait for the data, so many copies are in flight at once; completion is
+// awaited with cp_async_wait_all() and then a barrier.
+__device__ __forceinline__ void cp_async_4(float *smem_dst, const float *gmem_src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_16(float4 *smem_dst, const float4 *gmem_src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+
+
+// The block of B ids (B = 2, 4, 8) a lane reads for one row of a group, in
+// its natural width, and the contrib sum of one block.
+template <int B> struct IdBlock;
+template <> struct IdBlock<2> {
+  unsigned w;
+  __device__ __forceinline__ void load(const uint16_t *p, uint64_t pol) {
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
+        : "=r"(w) : "l"(p), "l"(pol));
+  }
+  __device__ __forceinline__ unsigned id(int k) const { return k ? (w >> 16) : (w & 0xffffu); }
+};
+template <> struct IdBlock<4> {
+  unsigned w0, w1;
+  __device__ __forceinline__ void load(const uint16_t *p, uint64_t pol) {
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
+        : "=r"(w0), "=r"(w1) : "l"(p), "l"(pol));
+  }
+  __device__ __forceinline__ unsigned id(int k) const {
+    const unsigned w = k < 2 ? w0 : w1;
+    return (k & 1) ? (w >> 16) : (w & 0xffffu);
+  }
+};
+template <> struct IdBlock<8> {
+  uint4 q;
+  __device__ __forceinline__ void load(const uint16_t *p, uint64_t pol) {
+    q = ld_stream_u4(reinterpret_cast<const uint4 *>(p), pol);
+  }
+  __device__ __forceinline__ unsigned id(int k) const {
+    const unsigned w = k < 2 ? q.x : (k < 4 ? q.y : (k < 6 ? q.z : q.w));
+    return (k & 1) ? (w >> 16) : (w & 0xffffu);
+  }
+};
+
+// A warp's contiguous block of ng groups of one run (all of one shape: rows
+// rows of 32 lanes x B ids, 2^ll lanes per pair) is one regular array: item
+// i (row i % rows of group i / rows) of lane l sits at base + (32 i + l) B.
+// Each lane streams its column with U items (32-64 bytes) in flight,
+// keeps B running sums (one per position in a block), and at the end of
+// each group joins them by a fixed tree, then across the pair's lanes by an
+// xor tree; the pair's first lane writes the partial to part[dest[32 g + p]].
+// dest is fetched one group ahead.
+template <int B>
+__device__ __forceinline__ void warp_run_groups(const BlockedArgs &a, const uint16_t *base,
+                                                int g, int ng, int rows, int ll, unsigned svb,
+                                                uint64_t pol) {
+  constexpr int U = B >= 4 ? 32 / B : 8;
+  const int lane = threadIdx.x & 31;
+  const int p = lane >> ll;
+  const int nitems = ng * rows;
+  const int gend = g + ng;
+  int d_next = ld_stream_s32(a.dest + static_cast<int64_t>(g) * 32 + p, pol);
+  float acc[B];
+#pragma unroll
+  for (int k = 0; k < B; k++) acc[k] = 0.f;
+  int row = 0;
+  const uint16_t *col = base + lane * B;
+  for (int i = 0; i < nitems; i += U) {
+    IdBlock<B> q[U];
+#pragma unroll
+    for (int t = 0; t < U; t++)
+      if (i + t < nitems) q[t].load(col + static_cast<int64_t>(i + t) * 32 * B, pol);
+#pragma unroll
+    for (int t = 0; t < U; t++) {
+      if (i + t >= nitems) break;
+#pragma unroll
+      for (int k = 0; k < B; k++) acc[k] = __fadd_rn(acc[k], lds_f32(svb, q[t].id(k)));
+      if (++row == rows) {
+        // the group is complete
+#pragma unroll
+        for (int h = B / 2; h > 0; h >>= 1)
+#pragma unroll
+          for (int k = 0; k < h; k++) acc[k] = __fadd_rn(acc[k], acc[k + h]);
+        float sum = acc[0];
+        for (int o = (1 << ll) >> 1; o > 0; o >>= 1)
+          sum = __fadd_rn(sum, __shfl_xor_sync(kFull, sum, o));
+        const int d = d_next;
+        if (g + 1 < gend) d_next = ld_stream_s32(a.dest + static_cast<int64_t>(g + 1) * 32 + p, pol);
+        // d is a position in part[] by construction; the range check keeps a
+        // layout fault from writing outside it
+        if ((lane & ((1 << ll) - 1)) == 0 &&
+            static_cast<unsigned>(d) < static_cast<unsigned>(a.part_len))
+          st_hint_f32(a.part + d, sum, pol);
+#pragma unroll
+        for (int k = 0; k < B; k++) acc[k] = 0.f;
+        row = 0;
+        g++;
+      }
+    }
+  }
+}
+
+// The same for runs whose pairs are one block each (lengths 1, 2, 4, 8:
+// rows = 1, one lane per pair): the warp's groups are a flat array of pairs
+// of B = 2^lb ids, pair j at base + j B with slot 32 g + j.  A lane takes
+// 16-byte chunks (8 ids: 8 / B pairs) two at a time with their dests; the
+// sum of a pair is a fixed tree over its ids (level lb of the pairwise tree
+// over the chunk), written to part[dest[slot]].
+__device__ __forceinline__ void warp_flat_pairs(const BlockedArgs &a, const uint16_t *base,
+                                                int g, int ng, int lb, unsigned svb,
+                                                uint64_t pol) {
+  const int lane = threadIdx.x & 31;
+  const int pp = 8 >> lb;             // pairs per chunk
+  const int nchunks = (ng * 32) >> (3 - lb);  // groups hold 32 pairs: whole chunks
+  const uint4 *c4 = reinterpret_cast<const uint4 *>(base);
+  const int32_t *dst = a.dest + static_cast<int64_t>(g) * 32;
+  for (int c0 = 0; c0 < nchunks; c0 += 2 * 32) {
+    uint4 q[2];
+    int d[2][8];
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const int c = c0 + t * 32 + lane;
+      if (c < nchunks) {
+        q[t] = ld_stream_u4(c4 + c, pol);
+        // the chunk's dests: 8, 4, 2 or 1 consecutive ints, aligned to their size
+        const int32_t *dp = dst + c * pp;
+        if (pp >= 4) {
+          const int4 d0 = ld_stream_v4(reinterpret_cast<const int4 *>(dp), pol);
+          d[t][0] = d0.x; d[t][1] = d0.y; d[t][2] = d0.z; d[t][3] = d0.w;
+          if (pp == 8) {
+            const int4 d1 = ld_stream_v4(reinterpret_cast<const int4 *>(dp + 4), pol);
+            d[t][4] = d1.x; d[t][5] = d1.y; d[t][6] = d1.z; d[t][7] = d1.w;
+          }
+        } else if (pp == 2) {
+          int2 d0;
+          asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.s32 {%0,%1}, [%2], %3;"
+              : "=r"(d0.x), "=r"(d0.y) : "l"(dp), "l"(pol));
+          d[t][0] = d0.x; d[t][1] = d0.y;
+        } else {
+          d[t][0] = ld_stream_s32(dp, pol);
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const int c = c0 + t * 32 + lane;
+      if (c >= nchunks) break;
+      const unsigned w[4] = {q[t].x, q[t].y, q[t].z, q[t].w};
+      float v[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+        v[k] = lds_f32(svb, (k & 1) ? (w[k >> 1] >> 16) : (w[k >> 1] & 0xffffu));
+      // pairwise tree: after level h, v[j << h] holds the sum of ids
+      // [j 2^h, (j + 1) 2^h)
+#pragma unroll
+      for (int h = 0; h < 3; h++) {
+        if (h >= lb) break;
+#pragma unroll
+        for (int j = 0; j < 8; j += 2 << h) v[j] = __fadd_rn(v[j], v[j + (1 << h)]);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        if (j >= pp) break;
+        const int dj = d[t][j];
+        // v[(j << lb) & 7], selected without indexing registers at run time
+        const float x = lb == 0 ? v[j] : (lb == 1 ? v[(2 * j) & 7] : (lb == 2 ? v[(4 * j) & 7] : v[0]));
+        if (static_cast<unsigned>(dj) < static_cast<unsigned>(a.part_len))
+          st_hint_f32(a.part + dj, x, pol);
+      }
+    }
+  }
+}
+
+// Phase 1: one CTA per SM takes units (a range of the groups of one (slice,
+// class) run) in order from a counter until none is left: the runs of one
+// block per pair (FLAT) or the others, the two kinds being two launches so
+// that each is compiled for its own paths.  When the slice changes the CTA
+// loads the slice's contribs into shared memory (plus a zero at index
+// slice_verts, the id of padding entries); each warp takes an equal share of
+// the unit's groups.
+template <bool FLAT>
+__global__ void __launch_bounds__(kSliceThreads, 1)
+slice_partial_kernel(const BlockedArgs a) {
+  if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
+  extern __shared__ __align__(16) float sv[];
+  __shared__ int s_unit;
+  const uint64_t ps = policy_evict_first();
+  const int w = threadIdx.x >> 5;
+  int cur_slice = -1;
+  const int ubase = FLAT ? 0 : a.nunits_flat;
+  const int ucount = FLAT ? a.nunits_flat : a.nunits - a.nunits_flat;
+  int *next = &a.ctl->unit_next[FLAT ? 0 : 1];
+  for (;;) {
+    if (threadIdx.x == 0) s_unit = atomicAdd(next, 1);
+    __syncthreads();  // also: every warp is done with the previous unit
+    const int k = s_unit;
+    if (k >= ucount) break;
+    const int4 un = a.unit[ubase + k];  // run, first group, end group
+    const int4 rd = a.run[un.x];        // first group, slice, first id, shape
+    if (rd.y != cur_slice) {
+      const int v0 = rd.y * a.slice_verts;
+      const int cnt = min(a.slice_verts, a.nsrc - v0);
+      const int n4 = cnt >> 2;
+      const float4 *c4 = reinterpret_cast<const float4 *>(a.contrib + v0);
+      float4 *sv4 = reinterpret_cast<float4 *>(sv);
+      for (int i = threadIdx.x; i < n4; i += kSliceThreads) cp_async_16(sv4 + i, c4 + i);
+      for (int i = (n4 << 2) + threadIdx.x; i < cnt; i += kSliceThreads)
+        cp_async_4(sv + i, a.contrib + v0 + i);
+      if (threadIdx.x == 0) sv[a.slice_verts] = 0.f;
+      cp_async_wait_all();
+      cur_slice = rd.y;
+    }
+    __syncthreads();  // the slice is in place; s_unit may be overwritten next
+    const int rows = rd.w >> 8, ll = (rd.w >> 4) & 15, lb = rd.w & 15;
+    const int ng = un.z - un.y;
+    const int per = (ng + kSliceWarps - 1) / kSliceWarps;
+    const int gw0 = un.y + w * per, gw1 = min(un.z, gw0 + per);
+    if (gw0 >= gw1) continue;
+    const uint16_t *base =
+        a.src + rd.z + (static_cast<int64_t>(gw0 - rd.x) * rows * 32 << lb);
+    const unsigned svb = smem_addr(sv);
+    if (FLAT) {
+      warp_flat_pairs(a, base, gw0, gw1 - gw0, lb, svb, ps);
+    } else {
+      switch (lb) {
+        case 1: warp_run_groups<2>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
+        case 2: warp_run_groups<4>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
+        default: warp_run_groups<8>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
+      }
+    }
+  }
+}
+
+// Phase 2: one CTA per bin of rows (then blocks for the rows without
+// in-edges, on the first sweep only).  The bin's partials, one contiguous
+// block of part[], are copied into shared memory; then each thread takes
+// rows u = row0 + t, + kBinThreads, ...: it sums the row's partials in slice
+// order (their positions in the block: idx[rowq[u] .. rowq[u + 1])) and
+// updates the row.
+__global__ void __launch_bounds__(kBinThreads)
+bin_row_kernel(const BlockedArgs a) {
+  if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
+  const int it = *reinterpret_cast<volatile const int *>(&a.ctl->loop.loops);
+  extern __shared__ __align__(16) float sm[];
+  __shared__ double sred[kBinWarps];
+  const uint64_t ps = policy_evict_first();
+  const uint64_t pl = policy_evict_last();
+  double err = 0.0;  // every |new - old| added in FP64 (src/pr_spmv.cc:42,53)
+  const int b = blockIdx.x;
+  // both phase-1 launches of this sweep are complete: their unit counters
+  // start again from zero for the next sweep
+  if (b == 0 && threadIdx.x == 0) a.ctl->unit_next[0] = a.ctl->unit_next[1] = 0;
+  if (b < a.nbins) {
+    const int4 bn = a.bin[b];
+    const int row0 = bn.x, row1 = bn.y, q0 = bn.z, q1 = bn.w;
+    const int np4 = (q1 - q0 + 3) >> 2;  // the block is padded to whole float4
+    const float4 *src4 = reinterpret_cast<const float4 *>(a.part + a.binbase[b]);
+    float4 *sm4 = reinterpret_cast<float4 *>(sm);
+    for (int i = threadIdx.x; i < np4; i += kBinThreads) cp_async_16(sm4 + i, src4 + i);
+    // the first row's own data is fetched while the block arrives
+    int u = row0 + threadIdx.x;
+    int s0 = 0, s1 = 0;
+    float old = 0.f;
+    if (u < row1) {
+      s0 = a.rowq[u];
+      s1 = a.rowq[u + 1];
+      old = ld_score(a.score + u, ps);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const unsigned smb = smem_addr(sm);
+    while (u < row1) {
+      float sum = 0.f;
+      int j = s0;
+      for (; j + 3 < s1; j += 4) {
+        const unsigned i0 = a.idx[j], i1 = a.idx[j + 1], i2 = a.idx[j + 2], i3 = a.idx[j + 3];
+        sum = __fadd_rn(sum, lds_f32(smb, i0));
+        sum = __fadd_rn(sum, lds_f32(smb, i1));
+        sum = __fadd_rn(sum, lds_f32(smb, i2));
+        sum = __fadd_rn(sum, lds_f32(smb, i3));
+      }
+      for (; j < s1; j++) sum = __fadd_rn(sum, lds_f32(smb, a.idx[j]));
+      const int un = u + kBinThreads;
+      int n0 = 0, n1 = 0;
+      float nold = 0.f;
+      if (un < row1) {  // the next row's data, fetched before this row is written
+        n0 = a.rowq[un];
+        n1 = a.rowq[un + 1];
+        nold = ld_score(a.score + un, ps);
+      }
+      const float base = a.kind == kKindPPR ? a.base_vec[u] : a.base_scalar;
+      // the reference's update: base + d * sum, two roundings (src/pr_spmv.cc:51)
+      const float nw = __fadd_rn(base, __fmul_rn(a.damping, sum));
+      st_hint_f32(a.score + u, nw, ps);
+      const int deg = a.odeg ? a.odeg[u] : a.rowoff[u + 1] - a.rowoff[u];
+      st_hint_f32(a.contrib + u, __fdiv_rn(nw, __int2float_rn(deg)), pl);
+      err += static_cast<double>(fabsf(__fsub_rn(nw, old)));
+      u = un;
+      s0 = n0;
+      s1 = n1;
+      old = nold;
+    }
+  } else if (it == 0) {
+    // rows without in-neighbours: new = base from the first sweep on
+    const int lo = a.ndst + (b - a.nbins) * kZeroRowsPerBlock;
+    const int hi = min(a.n, lo + kZeroRowsPerBlock);
+    for (int u = lo + threadIdx.x; u < hi; u += kBinThreads) {
+      const float base = a.kind == kKindPPR ? a.base_vec[u] : a.base_scalar;
+      const float nw = __fadd_rn(base, __fmul_rn(a.damping, 0.f));
+      const float old = ld_score(a.score + u, ps);
+      st_hint_f32(a.score + u, nw, ps);
+      // in a directed graph such a row can still have out-edges
+      if (a.odeg) st_hint_f32(a.contrib + u, __fdiv_rn(nw, __int2float_rn(a.odeg[u])), pl);
+      err += static_cast<double>(fabsf(__fsub_rn(nw, old)));
+    }
+  }
+  const double block_err = block_sum_d<kBinThreads>(err, sred);
+  const SweepReduce red{a.part1, a.part2, a.tick1, a.trace, a.ctl, a.nblocks, a.epsilon};
+  sweep_grid_finish<kBinThreads>(red, it, block_err, sred);
+}
+
+}  // namespace
+
+const void *SlicePartialKernel(bool flat) {
+  return flat ? reinterpret_cast<const void *>(slice_partial_kernel<true>)
+              : reinterpret_cast<const void *>(slice_partial_kernel<false>);
+}
+const void *BinRowKernel() { return reinterpret_cast<const void *>(bin_row_kernel); }
+
+int BinRowGrid(const SliceBlocks &sb, int64_t n) {
+  return sb.nbins + static_cast<int>((n - sb.ndst + kZeroRowsPerBlock - 1) / kZeroRowsPerBlock);
+}
+
+// contribs + the zero slot, rounded to whole float4
+size_t SliceSmemBytes(const SliceBlocks &sb) { return sizeof(float) * (sb.slice_verts + 4); }
+size_t BinSmemBytes(const SliceBlocks &sb) { return sizeof(float) * sb.bin_words; }
+
+}  // namespace prgpu

@@ -79,6 +79,7 @@ struct SweepCtl {
   LoopCtl loop;     // done flag + sweep index (see loop_graph.h)
   int sweeps;       // sweeps completed
   unsigned tick2;   // stage-2 ticket of the grid reduction
+  int unit_next[2]; // slice-blocked sweeps: phase-1 units taken (flat, other)
 };
 
 struct Scratch {

@@ -49,14 +49,12 @@ bool PlainLaunchMode() {
 void LoopGraph::Reset() {
   if (exec_) cudaGraphExecDestroy(exec_);
   exec_ = nullptr;
-  fn_ = nullptr;
-  args_.clear();
+  body_.clear();
   ctl_ = nullptr;
   max_iters_ = 0;
 }
 
-cudaError_t LoopGraph::Build(const void *fn, dim3 grid, dim3 block, const void *args,
-                             size_t args_size, LoopCtl *ctl, int max_iters) {
+cudaError_t LoopGraph::Build(const SweepKernel *ks, int nk, LoopCtl *ctl, int max_iters) {
   Reset();
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaGraphCreate(&g, 0);
@@ -73,19 +71,27 @@ cudaError_t LoopGraph::Build(const void *fn, dim3 grid, dim3 block, const void *
     cp.conditional.size = 1;
     e = cudaGraphAddNode(&loop_node, g, nullptr, 0, &cp);
   }
+  std::vector<Cached> body;
   if (e == cudaSuccess) {
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    std::vector<unsigned char> arg_copy(static_cast<const unsigned char *>(args),
-                                        static_cast<const unsigned char *>(args) + args_size);
-    void *sweep_params[] = {arg_copy.data()};
-    cudaKernelNodeParams kp = {};
-    kp.func = const_cast<void *>(fn);
-    kp.gridDim = grid;
-    kp.blockDim = block;
-    kp.sharedMemBytes = 0;
-    kp.kernelParams = sweep_params;
-    cudaGraphNode_t sweep_node = nullptr, decide_node = nullptr;
-    e = cudaGraphAddKernelNode(&sweep_node, body, nullptr, 0, &kp);
+    cudaGraph_t bg = cp.conditional.phGraph_out[0];
+    cudaGraphNode_t prev = nullptr;
+    for (int i = 0; i < nk && e == cudaSuccess; i++) {
+      Cached c{ks[i].fn, ks[i].grid, ks[i].block, ks[i].smem,
+               std::vector<unsigned char>(static_cast<const unsigned char *>(ks[i].args),
+                                          static_cast<const unsigned char *>(ks[i].args) +
+                                              ks[i].args_size)};
+      void *params[] = {c.args.data()};
+      cudaKernelNodeParams kp = {};
+      kp.func = const_cast<void *>(c.fn);
+      kp.gridDim = c.grid;
+      kp.blockDim = c.block;
+      kp.sharedMemBytes = static_cast<unsigned>(c.smem);
+      kp.kernelParams = params;
+      cudaGraphNode_t node = nullptr;
+      e = cudaGraphAddKernelNode(&node, bg, prev ? &prev : nullptr, prev ? 1 : 0, &kp);
+      prev = node;
+      body.push_back(std::move(c));
+    }
     if (e == cudaSuccess) {
       LoopCtl *c = ctl;
       int mi = max_iters;
@@ -96,7 +102,8 @@ cudaError_t LoopGraph::Build(const void *fn, dim3 grid, dim3 block, const void *
       dp.gridDim = dim3(1);
       dp.blockDim = dim3(32);
       dp.kernelParams = decide_params;
-      e = cudaGraphAddKernelNode(&decide_node, body, &sweep_node, 1, &dp);
+      cudaGraphNode_t decide_node = nullptr;
+      e = cudaGraphAddKernelNode(&decide_node, bg, prev ? &prev : nullptr, prev ? 1 : 0, &dp);
     }
   }
   if (e == cudaSuccess) e = cudaGraphInstantiate(&exec_, g, 0);
@@ -105,38 +112,60 @@ cudaError_t LoopGraph::Build(const void *fn, dim3 grid, dim3 block, const void *
     exec_ = nullptr;
     return e;
   }
-  fn_ = fn;
-  grid_ = grid;
-  block_ = block;
-  args_.assign(static_cast<const unsigned char *>(args),
-               static_cast<const unsigned char *>(args) + args_size);
+  body_ = std::move(body);
   ctl_ = ctl;
   max_iters_ = max_iters;
   return cudaSuccess;
 }
 
-cudaError_t LoopGraph::Launch(const void *fn, dim3 grid, dim3 block, const void *args,
-                              size_t args_size, LoopCtl *ctl, int max_iters, cudaStream_t s) {
+bool LoopGraph::Same(const SweepKernel *ks, int nk, LoopCtl *ctl, int max_iters) const {
+  if (!exec_ || ctl != ctl_ || max_iters != max_iters_ || static_cast<int>(body_.size()) != nk)
+    return false;
+  for (int i = 0; i < nk; i++) {
+    const Cached &c = body_[i];
+    if (c.fn != ks[i].fn || c.grid.x != ks[i].grid.x || c.block.x != ks[i].block.x ||
+        c.smem != ks[i].smem || c.args.size() != ks[i].args_size ||
+        std::memcmp(c.args.data(), ks[i].args, ks[i].args_size) != 0)
+      return false;
+  }
+  return true;
+}
+
+cudaError_t LoopGraph::Launch(const SweepKernel *ks, int nk, LoopCtl *ctl, int max_iters,
+                              cudaStream_t s) {
   if (max_iters < 1) return cudaSuccess;
   if (PlainLaunchMode()) {
-    std::vector<unsigned char> blob(static_cast<const unsigned char *>(args),
-                                    static_cast<const unsigned char *>(args) + args_size);
-    void *params[] = {blob.data()};
+    std::vector<std::vector<unsigned char>> blobs;
+    for (int k = 0; k < nk; k++)
+      blobs.emplace_back(static_cast<const unsigned char *>(ks[k].args),
+                         static_cast<const unsigned char *>(ks[k].args) + ks[k].args_size);
     for (int i = 0; i < max_iters; i++) {
-      cudaError_t e = cudaLaunchKernel(fn, grid, block, params, 0, s);
-      if (e != cudaSuccess) return e;
+      for (int k = 0; k < nk; k++) {
+        void *params[] = {blobs[k].data()};
+        cudaError_t e = cudaLaunchKernel(ks[k].fn, ks[k].grid, ks[k].block, params,
+                                         ks[k].smem, s);
+        if (e != cudaSuccess) return e;
+      }
       loop_advance_kernel<<<1, 32, 0, s>>>(ctl, max_iters);
     }
     return cudaGetLastError();
   }
-  const bool same = exec_ && fn == fn_ && grid.x == grid_.x && block.x == block_.x &&
-                    ctl == ctl_ && max_iters == max_iters_ && args_.size() == args_size &&
-                    std::memcmp(args_.data(), args, args_size) == 0;
-  if (!same) {
-    cudaError_t e = Build(fn, grid, block, args, args_size, ctl, max_iters);
+  if (!Same(ks, nk, ctl, max_iters)) {
+    cudaError_t e = Build(ks, nk, ctl, max_iters);
     if (e != cudaSuccess) return e;
   }
   return cudaGraphLaunch(exec_, s);
+}
+
+cudaError_t LoopGraph::Launch(const void *fn, dim3 grid, dim3 block, const void *args,
+                              size_t args_size, LoopCtl *ctl, int max_iters, cudaStream_t s) {
+  SweepKernel k;
+  k.fn = fn;
+  k.grid = grid;
+  k.block = block;
+  k.args = args;
+  k.args_size = args_size;
+  return Launch(&k, 1, ctl, max_iters, s);
 }
 
 }  // namespace prgpu

@@ -1,10 +1,10 @@
 // loop_graph.h -- a solve's sweep loop as one CUDA graph with a device-side
 // WHILE condition.
 //
-// Body = { sweep kernel, decide kernel }.  The sweep kernel reads the sweep
-// index from LoopCtl::loops and records convergence in LoopCtl::done; the
-// one-thread decide kernel then increments loops and sets the loop condition
-// to (!done && loops < max_iters).  The loop therefore ends after at most
+// Body = { sweep kernel(s), decide kernel }.  The sweep kernels read the
+// sweep index from LoopCtl::loops and the last one records convergence in
+// LoopCtl::done; the one-thread decide kernel then increments loops and sets
+// the loop condition to (!done && loops < max_iters).  The loop therefore ends after at most
 // max_iters bodies whatever the sweep kernel computes, and no launch is spent
 // after convergence.
 #ifndef GAPBS_B200_ENGINE_LOOP_GRAPH_H_
@@ -30,6 +30,16 @@ struct LoopCtl {
 // graphs with conditional nodes); results are identical.
 bool PlainLaunchMode();
 
+// One kernel of a sweep body: fn<<<grid, block, smem>>>(args), where args
+// points to the kernel's single by-value parameter of args_size bytes.
+struct SweepKernel {
+  const void *fn = nullptr;
+  dim3 grid, block;
+  size_t smem = 0;
+  const void *args = nullptr;
+  size_t args_size = 0;
+};
+
 class LoopGraph {
  public:
   LoopGraph() = default;
@@ -42,16 +52,24 @@ class LoopGraph {
   // launch shape, argument bytes, control block and max_iters are unchanged.
   cudaError_t Launch(const void *fn, dim3 grid, dim3 block, const void *args,
                      size_t args_size, LoopCtl *ctl, int max_iters, cudaStream_t s);
+  // The same for a body of several kernels run in order (then the decide
+  // kernel); the sweep index they read is the same within one body.
+  cudaError_t Launch(const SweepKernel *ks, int nk, LoopCtl *ctl, int max_iters,
+                     cudaStream_t s);
   void Reset();
 
  private:
-  cudaError_t Build(const void *fn, dim3 grid, dim3 block, const void *args,
-                    size_t args_size, LoopCtl *ctl, int max_iters);
+  cudaError_t Build(const SweepKernel *ks, int nk, LoopCtl *ctl, int max_iters);
+  bool Same(const SweepKernel *ks, int nk, LoopCtl *ctl, int max_iters) const;
 
+  struct Cached {
+    const void *fn;
+    dim3 grid, block;
+    size_t smem;
+    std::vector<unsigned char> args;
+  };
   cudaGraphExec_t exec_ = nullptr;
-  const void *fn_ = nullptr;
-  dim3 grid_, block_;
-  std::vector<unsigned char> args_;
+  std::vector<Cached> body_;
   LoopCtl *ctl_ = nullptr;
   int max_iters_ = 0;
 };

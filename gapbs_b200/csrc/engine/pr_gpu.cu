@@ -17,6 +17,7 @@
 
 #include "internal.h"
 #include "batched.h"
+#include "blocked.h"
 
 using prgpu::DeviceGraph;
 using prgpu::Scratch;
@@ -32,10 +33,18 @@ struct pr_gpu {
   prgpu::BatchScratch bsc;
   prgpu::LoopGraph loop_single;   // cached sweep-loop graphs
   prgpu::LoopGraph loop_adjoint;
+  prgpu::LoopGraph loop_blocked;
+  // slice-blocked layout of the uploaded graph (built at upload unless the
+  // layout is PR_GPU_SWEEP_GATHER) and the settings it was built with
+  prgpu::SliceBlocks sb;
+  int sweep_layout = PR_GPU_SWEEP_AUTO;
+  int slice_verts = 0, bin_words = 0;
+  bool sb_built = false;  // a build was attempted for the current graph and settings
   cudaEvent_t ev[4] = {};
   double last_sweep_ms = 0, last_total_ms = 0;
   int64_t last_launches = 0;
   int last_adjoint_sweeps = 0;
+  bool last_blocked = false;
   // pinned staging for host <-> device copies
   static constexpr size_t kChunk = 32u << 20;
   void *pinned[2] = {nullptr, nullptr};
@@ -298,12 +307,48 @@ int CheckRunArgs(pr_gpu_t *h, int max_iters, int ncols) {
   return PR_GPU_OK;
 }
 
+// Builds the slice-blocked layout of the current graph when the layout
+// setting asks for it.  Under PR_GPU_SWEEP_AUTO a graph outside the layout's
+// limits, or a device without room for it, keeps the gather sweep.
+int EnsureSliceBlocks(pr_gpu_t *h) {
+  if (h->sb_built || h->sweep_layout == PR_GPU_SWEEP_GATHER || !h->has_graph) return PR_GPU_OK;
+  h->sb_built = true;
+  h->loop_blocked.Reset();
+  std::string msg;
+  cudaError_t e = prgpu::BuildSliceBlocks(h->g, h->slice_verts, h->bin_words, &h->sb, h->stream,
+                                          &msg);
+  if (e == cudaSuccess) return PR_GPU_OK;
+  cudaGetLastError();
+  if (h->sweep_layout == PR_GPU_SWEEP_AUTO && e == cudaErrorMemoryAllocation) return PR_GPU_OK;
+  return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
+}
+
+// Drops everything derived from the uploaded graph before a new one arrives.
+void DropGraph(pr_gpu_t *h) {
+  h->has_graph = false;
+  prgpu::FreeSliceBlocks(&h->sb);
+  h->sb_built = false;
+  h->loop_blocked.Reset();
+  prgpu::FreeDeviceGraph(&h->g);
+}
+
+bool UseBlocked(const pr_gpu_t *h) {
+  return h->sweep_layout != PR_GPU_SWEEP_GATHER && h->sb.ready && !h->g.weighted;
+}
+
 // Single-column solve on device buffers.  tele_old: teleport in original ids
 // (device) or nullptr for the reference's uniform PageRank.  out_old: device
 // buffer for scores in original ids.
 int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
                 const float *tele_old, float *out_old, int32_t *sweeps_out, double *err_trace) {
   DeviceGraph &g = h->g;
+  int rc = EnsureSliceBlocks(h);
+  if (rc) return rc;
+  if (h->sweep_layout == PR_GPU_SWEEP_BLOCKED && !UseBlocked(h))
+    return SetErr(h, PR_GPU_EINVAL,
+                  "the slice-blocked sweep does not fit this graph (weighted, no edges, or more "
+                  "source slices than a bin holds)");
+  const bool blocked = UseBlocked(h);
   int32_t task_start[prgpu::kNumBins + 1];
   prgpu::PullTasks(g, task_start);
   prgpu::PullArgs probe;
@@ -312,8 +357,8 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
   probe.win = g.weighted ? g.win : nullptr;
   probe.odeg = (g.directed && !g.weighted) ? g.odeg : nullptr;
   const void *sweep_fn = prgpu::PullSweepKernel(probe);
-  const int nblocks = prgpu::PullGrid(sweep_fn);
-  int rc = EnsureScratch(h, g.n, 1, nblocks, max_iters);
+  const int nblocks = blocked ? prgpu::BinRowGrid(h->sb, g.n) : prgpu::PullGrid(sweep_fn);
+  rc = EnsureScratch(h, g.n, 1, nblocks, max_iters);
   if (rc) return rc;
   Scratch &sc = h->sc;
   cudaStream_t s = h->stream;
@@ -364,8 +409,64 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
   a.epsilon = epsilon;
   a.c0 = sc.contrib[0];
   a.c1 = sc.contrib[1];
+  prgpu::BlockedArgs ba;
+  prgpu::SweepKernel body[3];
+  if (blocked) {
+    const prgpu::SliceBlocks &sb = h->sb;
+    std::memset(&ba, 0, sizeof(ba));
+    ba.src = sb.src;
+    ba.run = sb.run;
+    ba.unit = sb.unit;
+    ba.nunits_flat = sb.nunits_flat;
+    ba.nunits = sb.nunits;
+    ba.dest = sb.dest;
+    ba.slice_verts = sb.slice_verts;
+    ba.nsrc = sb.nsrc;
+    ba.part = sb.part;
+    ba.part_len = sb.part_len;
+    ba.binbase = sb.binbase;
+    ba.idx = sb.idx;
+    ba.rowq = sb.rowq;
+    ba.bin = sb.bin;
+    ba.nbins = sb.nbins;
+    ba.n = static_cast<int32_t>(g.n);
+    ba.ndst = sb.ndst;
+    ba.zero_blocks = nblocks - sb.nbins;
+    ba.kind = a.kind;
+    ba.rowoff = g.rowoff;
+    ba.odeg = g.directed ? g.odeg : nullptr;
+    ba.base_vec = a.base_vec;
+    ba.base_scalar = a.base_scalar;
+    ba.damping = damping;
+    ba.score = sc.score;
+    ba.contrib = sc.contrib[0];
+    ba.part1 = sc.part1;
+    ba.part2 = sc.part2;
+    ba.tick1 = sc.tick1;
+    ba.trace = sc.trace;
+    ba.ctl = sc.ctl;
+    ba.nblocks = nblocks;
+    ba.epsilon = epsilon;
+    const void *kf = prgpu::SlicePartialKernel(true), *kr = prgpu::SlicePartialKernel(false);
+    const void *kb = prgpu::BinRowKernel();
+    for (const void *k : {kf, kr})
+      PR_CHECK(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(prgpu::SliceSmemBytes(sb))));
+    PR_CHECK(h, cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(prgpu::BinSmemBytes(sb))));
+    for (int i = 0; i < 3; i++) {
+      body[i].fn = i == 0 ? kf : (i == 1 ? kr : kb);
+      body[i].grid = dim3(i < 2 ? sb.nctas : nblocks);
+      body[i].block = dim3(i < 2 ? prgpu::kSliceThreads : prgpu::kBinThreads);
+      body[i].smem = i < 2 ? prgpu::SliceSmemBytes(sb) : prgpu::BinSmemBytes(sb);
+      body[i].args = &ba;
+      body[i].args_size = sizeof(ba);
+    }
+  }
   PR_CHECK(h, cudaEventRecord(h->ev[1], s));
-  if (nblocks > 0)
+  if (blocked)
+    PR_CHECK(h, h->loop_blocked.Launch(body, 3, &sc.ctl->loop, max_iters, s));
+  else if (nblocks > 0)
     PR_CHECK(h, h->loop_single.Launch(sweep_fn, dim3(nblocks),
                                       dim3(prgpu::kSweepThreads), &a, sizeof(a), &sc.ctl->loop,
                                       max_iters, s));
@@ -385,7 +486,9 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
   cudaEventElapsedTime(&ms_total, h->ev[0], h->ev[3]);
   h->last_sweep_ms = ms_sweep;
   h->last_total_ms = ms_total;
-  h->last_launches = launches + 2 * static_cast<int64_t>(ctl.loop.loops);  // sweep + decide
+  // per sweep: the sweep kernel(s) + the decide kernel
+  h->last_launches = launches + (blocked ? 4 : 2) * static_cast<int64_t>(ctl.loop.loops);
+  h->last_blocked = blocked;
   if (sweeps_out) *sweeps_out = max_iters ? ctl.sweeps : 0;
   if (err_trace)
     for (int i = 0; i < max_iters; i++) err_trace[i] = trace[i];
@@ -511,7 +614,7 @@ void pr_gpu_destroy(pr_gpu_t *h) {
   prgpu::FreeBfsScratch(&h->bfs);
   h->loop_single.Reset();
   h->loop_adjoint.Reset();
-  prgpu::FreeDeviceGraph(&h->g);
+  DropGraph(h);
   FreeScratch(&h->sc);
   prgpu::FreeBatchScratch(&h->bsc);
   for (int i = 0; i < 2; i++) {
@@ -537,8 +640,7 @@ int pr_gpu_generate(pr_gpu_t *h, int uniform, int scale, int degree, const int32
     return SetErr(h, PR_GPU_ERANGE, "graph exceeds int32 offsets");
   if (!uniform && !perm) return SetErr(h, PR_GPU_EINVAL, "R-MAT needs the vertex permutation");
   PR_CHECK(h, cudaSetDevice(h->device));
-  h->has_graph = false;
-  prgpu::FreeDeviceGraph(&h->g);
+  DropGraph(h);
   FreeGenerated(h);
   std::string msg;
   int64_t n = 0, m = 0;
@@ -557,6 +659,10 @@ int pr_gpu_generate(pr_gpu_t *h, int uniform, int scale, int degree, const int32
     return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
   }
   h->has_graph = true;
+  {
+    const int brc = EnsureSliceBlocks(h);
+    if (brc) return brc;
+  }
   if (n_out) *n_out = n;
   if (m_out) *m_out = m;
   return PR_GPU_OK;
@@ -637,8 +743,7 @@ int pr_gpu_upload_sg(pr_gpu_t *h, const char *path) {
     std::fclose(f);
     return CudaErr(h, e, "cudaSetDevice");
   }
-  h->has_graph = false;
-  prgpu::FreeDeviceGraph(&h->g);
+  DropGraph(h);
   FreeGenerated(h);
   int32_t *d_oo = nullptr, *d_on = nullptr, *d_io = nullptr, *d_in = nullptr;
   int64_t *wide = nullptr;
@@ -690,7 +795,7 @@ int pr_gpu_upload_sg(pr_gpu_t *h, const char *path) {
     return SetErr(h, PR_GPU_EGRAPH, msg);
   if (e != cudaSuccess) return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
   h->has_graph = true;
-  return PR_GPU_OK;
+  return EnsureSliceBlocks(h);
 }
 
 int pr_gpu_connected_components_device(pr_gpu_t *h, int32_t *comp_out_dev) {
@@ -770,8 +875,7 @@ int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m, const int32_t *out_off,
   const bool directed = in_off && (in_off != out_off || in_nbr != out_nbr);
   if (directed && m > 0 && !in_nbr) return SetErr(h, PR_GPU_EINVAL, "null in-CSR array");
   PR_CHECK(h, cudaSetDevice(h->device));
-  h->has_graph = false;
-  prgpu::FreeDeviceGraph(&h->g);
+  DropGraph(h);
   FreeGenerated(h);
   int32_t *d_oo = nullptr, *d_on = nullptr, *d_io = nullptr, *d_in = nullptr;
   float *d_w = nullptr;
@@ -807,7 +911,7 @@ int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m, const int32_t *out_off,
     return SetErr(h, PR_GPU_EGRAPH, msg);
   if (e != cudaSuccess) return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA, msg);
   h->has_graph = true;
-  return PR_GPU_OK;
+  return EnsureSliceBlocks(h);
 }
 
 int pr_gpu_run_device(pr_gpu_t *h, int max_iters, double epsilon, float damping, int ncols,
@@ -907,6 +1011,48 @@ int pr_gpu_set_batch_tile(pr_gpu_t *h, int width) {
 int pr_gpu_get_batch_tile(const pr_gpu_t *h, int *width) {
   if (!h || !width) return PR_GPU_EINVAL;
   *width = h->bsc.tile ? h->bsc.tile : h->bsc.tuned_tile;
+  return PR_GPU_OK;
+}
+
+int pr_gpu_set_sweep_layout(pr_gpu_t *h, int layout, int slice_verts, int bin_words) {
+  if (!h) return PR_GPU_EINVAL;
+  if (layout < PR_GPU_SWEEP_AUTO || layout > PR_GPU_SWEEP_BLOCKED)
+    return SetErr(h, PR_GPU_EINVAL, "sweep layout must be AUTO, GATHER or BLOCKED");
+  if (slice_verts != 0 &&
+      (slice_verts < 64 || slice_verts > prgpu::kMaxSliceVerts || slice_verts % 64 != 0))
+    return SetErr(h, PR_GPU_EINVAL, "slice_verts must be 0 or a multiple of 64 in [64, 56320]");
+  if (bin_words != 0 && (bin_words < 1024 || bin_words > prgpu::kMaxBinWords))
+    return SetErr(h, PR_GPU_EINVAL, "bin_words must be 0 or in [1024, 28160]");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  const bool rebuild = slice_verts != h->slice_verts || bin_words != h->bin_words ||
+                       (layout != PR_GPU_SWEEP_GATHER && !h->sb.ready);
+  h->sweep_layout = layout;
+  h->slice_verts = slice_verts;
+  h->bin_words = bin_words;
+  if (rebuild) {
+    PR_CHECK(h, cudaStreamSynchronize(h->stream));
+    prgpu::FreeSliceBlocks(&h->sb);
+    h->loop_blocked.Reset();
+    h->sb_built = false;
+  }
+  return PR_GPU_OK;
+}
+
+int pr_gpu_sweep_layout_info(pr_gpu_t *h, int *blocked, int *slices, int *bins, int64_t *pairs,
+                             int64_t *ids, int64_t *bytes, int *last_blocked) {
+  if (!h) return PR_GPU_EINVAL;
+  if (!h->has_graph) return SetErr(h, PR_GPU_ENOGRAPH, "no graph uploaded");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  int rc = EnsureSliceBlocks(h);
+  if (rc) return rc;
+  const bool on = UseBlocked(h);
+  if (blocked) *blocked = on ? 1 : 0;
+  if (slices) *slices = on ? h->sb.nslices : 0;
+  if (bins) *bins = on ? h->sb.nbins : 0;
+  if (pairs) *pairs = on ? h->sb.npairs : 0;
+  if (ids) *ids = on ? h->sb.elems : 0;
+  if (bytes) *bytes = on ? static_cast<int64_t>(h->sb.bytes) : 0;
+  if (last_blocked) *last_blocked = h->last_blocked ? 1 : 0;
   return PR_GPU_OK;
 }
 

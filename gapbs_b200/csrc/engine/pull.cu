@@ -26,6 +26,7 @@
 
 #include "common.cuh"
 #include "internal.h"
+#include "sweep_reduce.cuh"
 
 namespace prgpu {
 
@@ -146,44 +147,8 @@ __device__ __forceinline__ float finish_row(const PullArgs &a, float *cout, int 
 // block records the sweep's error and the convergence decision.
 __device__ __forceinline__ void grid_finish(const PullArgs &a, int it, double block_err,
                                             double *sred) {
-  __shared__ int s_last;
-  const int b = blockIdx.x;
-  const int g = b / kReduceGroup;
-  const int gsize = min(kReduceGroup, a.nblocks - g * kReduceGroup);
-  const int ngroups = (a.nblocks + kReduceGroup - 1) / kReduceGroup;
-  if (threadIdx.x == 0) {
-    a.part1[b] = block_err;
-    __threadfence();
-    const unsigned t = atomicAdd(&a.tick1[g], 1u);
-    s_last = (t == static_cast<unsigned>(gsize - 1));
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  double v = 0;
-  for (int i = threadIdx.x; i < gsize; i += blockDim.x)
-    v += __ldcg(a.part1 + g * kReduceGroup + i);
-  double tot = block_sum_d<kSweepThreads>(v, sred);
-  if (threadIdx.x == 0) {
-    a.part2[g] = tot;
-    a.tick1[g] = 0;
-    __threadfence();
-    const unsigned t2 = atomicAdd(&a.ctl->tick2, 1u);
-    s_last = (t2 == static_cast<unsigned>(ngroups - 1));
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  v = 0;
-  for (int i = threadIdx.x; i < ngroups; i += blockDim.x) v += __ldcg(a.part2 + i);
-  tot = block_sum_d<kSweepThreads>(v, sred);
-  if (threadIdx.x == 0) {
-    a.trace[it] = tot;
-    a.ctl->sweeps = it + 1;
-    a.ctl->tick2 = 0;
-    if (tot < a.epsilon) a.ctl->loop.done = 1;
-    __threadfence();
-  }
+  const SweepReduce r{a.part1, a.part2, a.tick1, a.trace, a.ctl, a.nblocks, a.epsilon};
+  sweep_grid_finish<kSweepThreads>(r, it, block_err, sred);
 }
 
 // One warp task of a G-lane-group bin: rows bin_row[bin] + task * (32 / G)

@@ -15,7 +15,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import byref, c_double, c_int64
+from ctypes import byref, c_double, c_int, c_int64
 from dataclasses import dataclass
 from typing import Optional
 
@@ -276,6 +276,26 @@ class PageRankEngine:
         w = ctypes.c_int()
         self._check(self._lib.pr_gpu_get_batch_tile(self._h, byref(w)), "pr_gpu_get_batch_tile")
         return w.value
+
+    def set_sweep_layout(self, layout: str = "auto", slice_verts: int = 0, bin_words: int = 0):
+        """Sweep layout of single-column solves on unweighted graphs:
+        "auto" (slice-blocked when the graph fits it), "gather" or "blocked";
+        slice_verts / bin_words 0 keep the defaults (see pr_gpu_set_sweep_layout)."""
+        code = {"auto": _pr_abi.PR_GPU_SWEEP_AUTO, "gather": _pr_abi.PR_GPU_SWEEP_GATHER,
+                "blocked": _pr_abi.PR_GPU_SWEEP_BLOCKED}[layout]
+        self._check(self._lib.pr_gpu_set_sweep_layout(self._h, code, int(slice_verts),
+                                                      int(bin_words)), "pr_gpu_set_sweep_layout")
+
+    def sweep_layout_info(self) -> dict:
+        on, sl, bn, last = c_int(), c_int(), c_int(), c_int()
+        pairs, ids, nbytes = c_int64(), c_int64(), c_int64()
+        self._check(self._lib.pr_gpu_sweep_layout_info(self._h, byref(on), byref(sl), byref(bn),
+                                                       byref(pairs), byref(ids), byref(nbytes),
+                                                       byref(last)),
+                    "pr_gpu_sweep_layout_info")
+        return {"blocked": bool(on.value), "slices": sl.value, "bins": bn.value,
+                "pairs": pairs.value, "ids": ids.value, "bytes": nbytes.value,
+                "last_run_blocked": bool(last.value)}
 
     def set_stream(self, stream_handle: Optional[int]):
         """Issue work on a caller stream (raw cudaStream_t), None = own stream."""

@@ -193,6 +193,38 @@ int pr_gpu_adjoint_device(pr_gpu_t *h, int max_iters, double epsilon,
 int pr_gpu_set_batch_tile(pr_gpu_t *h, int width);
 int pr_gpu_get_batch_tile(const pr_gpu_t *h, int *width);
 
+/* Sweep layout of single-column solves (plain and personalized PageRank) on
+ * unweighted graphs:
+ *   PR_GPU_SWEEP_AUTO     slice-blocked when the graph fits that layout's
+ *                         limits and the device has room for it, else gather
+ *   PR_GPU_SWEEP_GATHER   one sweep kernel that gathers contrib[v] for every
+ *                         in-edge (no extra device memory)
+ *   PR_GPU_SWEEP_BLOCKED  slice-blocked; a run on a graph it does not fit
+ *                         returns PR_GPU_EINVAL
+ * The slice-blocked sweep is two kernels per sweep: per slice of
+ * slice_verts consecutive source vertices (held in shared memory) a partial
+ * sum for every destination row the slice reaches, then per bin of rows
+ * (bin_words shared-memory words of partials and row sums) the row update.
+ * It holds about 2.3 bytes per edge and 14 bytes per (row, slice) pair of
+ * extra device memory, built from the device CSR at upload.  slice_verts
+ * (multiple of 64, 64..56320) and bin_words (1024..28160): 0 keeps the
+ * defaults (49152, 12288).  Changing them rebuilds the layout at the next
+ * run.  Weighted graphs, the adjoint and batched solves use gather sweeps.
+ * No counterpart in the reference. */
+#define PR_GPU_SWEEP_AUTO 0
+#define PR_GPU_SWEEP_GATHER 1
+#define PR_GPU_SWEEP_BLOCKED 2
+int pr_gpu_set_sweep_layout(pr_gpu_t *h, int layout, int slice_verts, int bin_words);
+
+/* The layout of the uploaded graph: *blocked = 1 when single-column solves
+ * use the slice-blocked sweep; its slice count, bin count, (row, slice)
+ * pairs, stored source ids (the edges plus padding) and device bytes (all
+ * nullable; 0 when not built).  *last_blocked: whether the last
+ * single-column run used it. */
+int pr_gpu_sweep_layout_info(pr_gpu_t *h, int *blocked, int *slices, int *bins,
+                             int64_t *pairs, int64_t *ids, int64_t *bytes,
+                             int *last_blocked);
+
 /* Makes the handle issue its work on `stream` (a cudaStream_t of the
  * handle's device, e.g. the caller's framework stream) instead of its own;
  * NULL restores the handle's own stream.  The handle does not take

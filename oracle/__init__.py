@@ -57,6 +57,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_ppr_f64.restype = c_int
         L.oracle_ppr_f64_from.argtypes = [c_int64, P, P, P, P, P, c_double, P, P, c_int, c_double, P, P]
         L.oracle_ppr_f64_from.restype = c_int
+        L.oracle_pr_rounding_f32.argtypes = [c_int64, P, P, P, c_int, c_float, P]
+        L.oracle_pr_rounding_f32.restype = None
         L.oracle_ppr_adjoint_f64.argtypes = [c_int64, P, P, P, c_double, P, P, c_int, c_double, P, P, P]
         L.oracle_ppr_adjoint_f64.restype = c_int
         _lib = L
@@ -90,6 +92,16 @@ def pr_pull_f64(g, max_iters=20, epsilon=1e-4, damping=0.85):
     k = lib().oracle_pr_pull_f64(n, _ptr(io), _ptr(inb), _ptr(oo), max_iters, epsilon,
                                  damping, _ptr(s), _ptr(tr))
     return s, k, tr[:k].copy()
+
+
+def pr_rounding_f32(g, nsweeps, damping=0.85):
+    """Per sweep, L1 distance of the reference's FP32 scores from FP64 Jacobi
+    run side by side from the same start (the reference's own rounding)."""
+    n, io, inb, oo, _ = _csr(g)
+    l1 = np.zeros(max(nsweeps, 1), np.float64)
+    lib().oracle_pr_rounding_f32(n, _ptr(io), _ptr(inb), _ptr(oo), int(nsweeps), damping,
+                                 _ptr(l1))
+    return l1[:nsweeps].copy()
 
 
 def pr_verify_f32(g, scores, damping=0.85) -> float:

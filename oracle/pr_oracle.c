@@ -47,6 +47,47 @@ int oracle_pr_pull_f32(int64_t n, const int64_t *in_off, const int32_t *in_nbr,
   return sweeps;
 }
 
+/* The reference's own rounding error per sweep: the FP32 mirror of
+ * src/pr_spmv.cc:35-61 and the same Jacobi sweeps in double, run side by
+ * side from the same start for exactly nsweeps sweeps (no stop test);
+ * l1[k] = sum_u |s32_k[u] - s64_k[u]| after sweep k. */
+void oracle_pr_rounding_f32(int64_t n, const int64_t *in_off, const int32_t *in_nbr,
+                            const int64_t *out_off, int nsweeps, float damping, double *l1) {
+  const float init32 = 1.0f / (float)n, base32 = (1.0f - damping) / (float)n;
+  const double init64 = 1.0 / (double)n, base64 = (1.0 - (double)damping) / (double)n;
+  const size_t cap = (size_t)(n > 0 ? n : 1);
+  float *s32 = (float *)malloc(sizeof(float) * cap), *c32 = (float *)malloc(sizeof(float) * cap);
+  double *s64 = (double *)malloc(sizeof(double) * cap), *c64 = (double *)malloc(sizeof(double) * cap);
+  for (int64_t u = 0; u < n; u++) {
+    s32[u] = init32;
+    s64[u] = init64;
+  }
+  for (int k = 0; k < nsweeps; k++) {
+    for (int64_t v = 0; v < n; v++) {
+      const int64_t d = deg_of(out_off, v);
+      c32[v] = s32[v] / (float)d;
+      c64[v] = d ? s64[v] / (double)d : 0.0;
+    }
+    double acc = 0;
+    for (int64_t u = 0; u < n; u++) {
+      float t32 = 0;
+      double t64 = 0;
+      for (int64_t e = in_off[u]; e < in_off[u + 1]; e++) {
+        t32 += c32[in_nbr[e]];
+        t64 += c64[in_nbr[e]];
+      }
+      s32[u] = base32 + damping * t32;
+      s64[u] = base64 + (double)damping * t64;
+      acc += fabs((double)s32[u] - s64[u]);
+    }
+    l1[k] = acc;
+  }
+  free(s32);
+  free(c32);
+  free(s64);
+  free(c64);
+}
+
 /* src/pr_spmv.cc:35-61 with double everywhere */
 int oracle_pr_pull_f64(int64_t n, const int64_t *in_off, const int32_t *in_nbr,
                        const int64_t *out_off, int max_iters, double epsilon,

@@ -38,6 +38,10 @@ int oracle_pr_pull_f32(int64_t n, const int64_t *in_off, const int32_t *in_nbr,
                        float damping, float *scores, double *err_trace);
 
 /* Same algorithm with every quantity in double.  Returns sweeps. */
+/* L1 distance of the FP32 mirror's scores from FP64 Jacobi after each of
+ * nsweeps sweeps from the same start (the reference's rounding per sweep). */
+void oracle_pr_rounding_f32(int64_t n, const int64_t *in_off, const int32_t *in_nbr,
+                            const int64_t *out_off, int nsweeps, float damping, double *l1);
 int oracle_pr_pull_f64(int64_t n, const int64_t *in_off, const int32_t *in_nbr,
                        const int64_t *out_off, int max_iters, double epsilon,
                        double damping, double *scores, double *err_trace);

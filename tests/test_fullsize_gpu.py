@@ -60,11 +60,15 @@ def load(case):
     return g, e
 
 
+@pytest.mark.parametrize("layout", ["blocked", "gather"])
 @pytest.mark.parametrize("case", ["u24", "g25"])
-def test_pagerankpull_fullsize(engine, case):
+def test_pagerankpull_fullsize(engine, case, layout):
     g, e = load(case)
+    engine.set_sweep_layout("auto" if layout == "blocked" else "gather")
     engine.upload(g)
     res = engine.run(20, 1e-4, 0.85)
+    assert engine.sweep_layout_info()["last_run_blocked"] == (layout == "blocked")
+    engine.set_sweep_layout("auto")
     s = res.scores
     # the reference's sweep count and its printed per-sweep L1 change
     assert int(res.sweeps[0]) == e["sweeps"]
