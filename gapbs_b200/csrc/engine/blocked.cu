@@ -150,51 +150,36 @@ __device__ __forceinline__ void warp_run_groups(const BlockedArgs &a, const uint
   }
 }
 
-// The same for runs whose pairs are one block each (lengths 1, 2, 4, 8:
-// rows = 1, one lane per pair): the warp's groups are a flat array of pairs
-// of B = 2^lb ids, pair j at base + j B with slot 32 g + j.  A lane takes
-// 16-byte chunks (8 ids: 8 / B pairs) two at a time with their dests; the
-// sum of a pair is a fixed tree over its ids (level lb of the pairwise tree
-// over the chunk), written to part[dest[slot]].
+// A warp's share of a flat run: blocks of 32 chunks of 16 bytes (8 ids),
+// chunk c holding pairs c, c + 32, ... (8 / B pairs of B ids) of the block.
+// Two blocks per step: every lane loads its chunk and the dests of its
+// pairs (one coalesced load per pair place), sums each pair's B ids and
+// stores the partials, each store lane-consecutive over the block's pairs.
 __device__ __forceinline__ void warp_flat_pairs(const BlockedArgs &a, const uint16_t *base,
                                                 int g, int ng, int lb, unsigned svb,
                                                 uint64_t pol) {
   const int lane = threadIdx.x & 31;
-  const int pp = 8 >> lb;             // pairs per chunk
-  const int nchunks = (ng * 32) >> (3 - lb);  // groups hold 32 pairs: whole chunks
+  const int pp = 8 >> lb;      // pairs per chunk
+  const int nblk = ng / pp;    // a block is pp groups (whole by the layout)
   const uint4 *c4 = reinterpret_cast<const uint4 *>(base);
   const int32_t *dst = a.dest + static_cast<int64_t>(g) * 32;
-  for (int c0 = 0; c0 < nchunks; c0 += 2 * 32) {
+  for (int b0 = 0; b0 < nblk; b0 += 2) {
     uint4 q[2];
     int d[2][8];
 #pragma unroll
     for (int t = 0; t < 2; t++) {
-      const int c = c0 + t * 32 + lane;
-      if (c < nchunks) {
-        q[t] = ld_stream_u4(c4 + c, pol);
-        // the chunk's dests: 8, 4, 2 or 1 consecutive ints, aligned to their size
-        const int32_t *dp = dst + c * pp;
-        if (pp >= 4) {
-          const int4 d0 = ld_stream_v4(reinterpret_cast<const int4 *>(dp), pol);
-          d[t][0] = d0.x; d[t][1] = d0.y; d[t][2] = d0.z; d[t][3] = d0.w;
-          if (pp == 8) {
-            const int4 d1 = ld_stream_v4(reinterpret_cast<const int4 *>(dp + 4), pol);
-            d[t][4] = d1.x; d[t][5] = d1.y; d[t][6] = d1.z; d[t][7] = d1.w;
-          }
-        } else if (pp == 2) {
-          int2 d0;
-          asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.s32 {%0,%1}, [%2], %3;"
-              : "=r"(d0.x), "=r"(d0.y) : "l"(dp), "l"(pol));
-          d[t][0] = d0.x; d[t][1] = d0.y;
-        } else {
-          d[t][0] = ld_stream_s32(dp, pol);
-        }
+      const int bk = b0 + t;
+      if (bk < nblk) {
+        q[t] = ld_stream_u4(c4 + bk * 32 + lane, pol);
+        const int32_t *dp = dst + bk * 32 * pp + lane;
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+          if (k < pp) d[t][k] = ld_stream_s32(dp + 32 * k, pol);
       }
     }
 #pragma unroll
     for (int t = 0; t < 2; t++) {
-      const int c = c0 + t * 32 + lane;
-      if (c >= nchunks) break;
+      if (b0 + t >= nblk) break;
       const unsigned w[4] = {q[t].x, q[t].y, q[t].z, q[t].w};
       float v[8];
 #pragma unroll
@@ -263,7 +248,9 @@ slice_partial_kernel(const BlockedArgs a) {
     __syncthreads();  // the slice is in place; s_unit may be overwritten next
     const int rows = rd.w >> 8, ll = (rd.w >> 4) & 15, lb = rd.w & 15;
     const int ng = un.z - un.y;
-    const int per = (ng + kSliceWarps - 1) / kSliceWarps;
+    // warps split the unit evenly, flat units in whole blocks of 8 / B groups
+    const int q = FLAT ? 8 >> lb : 1;
+    const int per = (ng / q + kSliceWarps - 1) / kSliceWarps * q;
     const int gw0 = un.y + w * per, gw1 = min(un.z, gw0 + per);
     if (gw0 >= gw1) continue;
     const uint16_t *base =
@@ -283,10 +270,11 @@ slice_partial_kernel(const BlockedArgs a) {
 
 // Phase 2: one CTA per bin of rows (then blocks for the rows without
 // in-edges, on the first sweep only).  The bin's partials, one contiguous
-// block of part[], are copied into shared memory; then each thread takes
-// rows u = row0 + t, + kBinThreads, ...: it sums the row's partials in slice
-// order (their positions in the block: idx[rowq[u] .. rowq[u + 1])) and
-// updates the row.
+// block of part[], are copied into shared memory (blk); the bin's stretch
+// of idx[] (its pairs in row order, each a position in the block) is
+// streamed with coalesced 16-byte loads and turned into the partials in row
+// order (ord); then each thread takes rows u = row0 + t, + kBinThreads, ...
+// and sums the row's stretch of ord in slice order.
 __global__ void __launch_bounds__(kBinThreads)
 bin_row_kernel(const BlockedArgs a) {
   if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
@@ -303,39 +291,71 @@ bin_row_kernel(const BlockedArgs a) {
   if (b < a.nbins) {
     const int4 bn = a.bin[b];
     const int row0 = bn.x, row1 = bn.y, q0 = bn.z, q1 = bn.w;
-    const int np4 = (q1 - q0 + 3) >> 2;  // the block is padded to whole float4
+    const int np = q1 - q0;
+    const int np4 = (np + 3) >> 2;  // the block is padded to whole float4
+    float *blk = sm;                // the bin's partials, block order
+    float *ord = sm + 4 * np4;      // the same, in (row, slice) order (16-byte aligned)
     const float4 *src4 = reinterpret_cast<const float4 *>(a.part + a.binbase[b]);
-    float4 *sm4 = reinterpret_cast<float4 *>(sm);
-    for (int i = threadIdx.x; i < np4; i += kBinThreads) cp_async_16(sm4 + i, src4 + i);
+    float4 *blk4 = reinterpret_cast<float4 *>(blk);
+    for (int i = threadIdx.x; i < np4; i += kBinThreads) cp_async_16(blk4 + i, src4 + i);
     // the first row's own data is fetched while the block arrives
     int u = row0 + threadIdx.x;
     int s0 = 0, s1 = 0;
     float old = 0.f;
     if (u < row1) {
-      s0 = a.rowq[u];
-      s1 = a.rowq[u + 1];
+      s0 = a.rowq[u] - q0;
+      s1 = a.rowq[u + 1] - q0;
       old = ld_score(a.score + u, ps);
+    }
+    // idx[q0 .. q1): 8 positions per 16-byte load; the stretch's first and
+    // last loads are masked to it
+    const int e0 = q0 & ~7, e1 = (q1 + 7) & ~7;
+    const int nq = (e1 - e0) >> 3;
+    uint4 iq[4];
+    const uint4 *idx4 = reinterpret_cast<const uint4 *>(a.idx + e0);
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const int c = threadIdx.x + t * kBinThreads;
+      if (c < nq) iq[t] = ld_stream_u4(idx4 + c, ps);
     }
     cp_async_wait_all();
     __syncthreads();
-    const unsigned smb = smem_addr(sm);
+    const unsigned blkb = smem_addr(blk);
+    // ord[j - e0] holds pair j's partial: each thread writes its 8 as two
+    // aligned 16-byte stores (entries outside [q0, q1) get a zero)
+    for (int c0 = 0; c0 < nq; c0 += 4 * kBinThreads) {
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        const int c = c0 + threadIdx.x + t * kBinThreads;
+        if (c >= nq) break;
+        const unsigned w[4] = {iq[t].x, iq[t].y, iq[t].z, iq[t].w};
+        float v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int j = e0 + c * 8 + k;  // pair number in the stream
+          v[k] = (j >= q0 && j < q1)
+                     ? lds_f32(blkb, (k & 1) ? (w[k >> 1] >> 16) : (w[k >> 1] & 0xffffu))
+                     : 0.f;
+        }
+        float4 *o4 = reinterpret_cast<float4 *>(ord) + 2 * c;
+        o4[0] = make_float4(v[0], v[1], v[2], v[3]);
+        o4[1] = make_float4(v[4], v[5], v[6], v[7]);
+        const int cn = c + 4 * kBinThreads;
+        if (cn < nq) iq[t] = ld_stream_u4(idx4 + cn, ps);
+      }
+    }
+    __syncthreads();
+    const unsigned ordb = smem_addr(ord) + 4u * static_cast<unsigned>(q0 - e0);
     while (u < row1) {
       float sum = 0.f;
-      int j = s0;
-      for (; j + 3 < s1; j += 4) {
-        const unsigned i0 = a.idx[j], i1 = a.idx[j + 1], i2 = a.idx[j + 2], i3 = a.idx[j + 3];
-        sum = __fadd_rn(sum, lds_f32(smb, i0));
-        sum = __fadd_rn(sum, lds_f32(smb, i1));
-        sum = __fadd_rn(sum, lds_f32(smb, i2));
-        sum = __fadd_rn(sum, lds_f32(smb, i3));
-      }
-      for (; j < s1; j++) sum = __fadd_rn(sum, lds_f32(smb, a.idx[j]));
+#pragma unroll 4
+      for (int j = s0; j < s1; j++) sum = __fadd_rn(sum, lds_f32(ordb, j));
       const int un = u + kBinThreads;
       int n0 = 0, n1 = 0;
       float nold = 0.f;
       if (un < row1) {  // the next row's data, fetched before this row is written
-        n0 = a.rowq[un];
-        n1 = a.rowq[un + 1];
+        n0 = a.rowq[un] - q0;
+        n1 = a.rowq[un + 1] - q0;
         nold = ld_score(a.score + un, ps);
       }
       const float base = a.kind == kKindPPR ? a.base_vec[u] : a.base_scalar;
@@ -383,6 +403,7 @@ int BinRowGrid(const SliceBlocks &sb, int64_t n) {
 
 // contribs + the zero slot, rounded to whole float4
 size_t SliceSmemBytes(const SliceBlocks &sb) { return sizeof(float) * (sb.slice_verts + 4); }
-size_t BinSmemBytes(const SliceBlocks &sb) { return sizeof(float) * sb.bin_words; }
+// the bin's partials twice (block order; row order from a multiple of 8)
+size_t BinSmemBytes(const SliceBlocks &sb) { return sizeof(float) * (2 * sb.bin_words + 16); }
 
 }  // namespace prgpu

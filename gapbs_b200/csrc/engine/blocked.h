@@ -48,10 +48,10 @@ namespace prgpu {
 constexpr int kSliceWarps = 32;
 constexpr int kBinWarps = 8;
 constexpr int kDefaultSliceVerts = 49152;  // 192 KB of contribs in shared memory
-constexpr int kDefaultBinWords = 6144;     // 24 KB of partials per bin (pairs + rows)
+constexpr int kDefaultBinWords = 6144;     // partials per bin (pairs + rows): 2 x 24 KB of shared memory
 constexpr int kMaxSliceVerts = 56320;      // + the zero slot, within one CTA's shared memory
 constexpr int kMaxPairIds = 2048;          // longer (row, slice) pairs are cut into pieces
-constexpr int kMaxBinWords = 28160;
+constexpr int kMaxBinWords = 28160;        // two copies of a bin's partials in shared memory
 struct SliceBlocks {
   bool ready = false;
   int32_t slice_verts = 0;   // source ids per slice

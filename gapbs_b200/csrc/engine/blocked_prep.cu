@@ -258,15 +258,32 @@ __global__ void run_start_kernel(int64_t npairs, const int32_t *__restrict__ fla
   run_start[run_incl[i] - 1] = static_cast<int32_t>(i);
 }
 
-// Groups of each (slice, class) run: its pairs, 32 / lanes to a group.
+// Runs of one block per pair (rows 1, one lane per pair) go to the flat
+// launch of phase 1.
+__host__ __device__ inline bool FlatShape(int code) { return (code >> 4) == 16; }
+
+// Classes whose runs have one block of B ids per pair and one lane per pair
+// (exact lengths 1, 2, 4 and 8): their runs are flat (FlatShape above).
+__host__ __device__ inline bool ClassFlat(int cls) {
+  return cls == 0 || cls == 1 || cls == 3 || cls == 7;
+}
+
+// Groups of each (slice, class) run: its pairs, 32 / lanes to a group; a
+// flat run is padded to whole blocks of 8 / B groups (32 chunks of 16 bytes).
 __global__ void run_groups_kernel(int32_t nruns, int64_t npairs,
                                   const int32_t *__restrict__ run_start,
                                   const uint32_t *__restrict__ key, int32_t *run_groups) {
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= nruns) return;
   const int64_t end = r + 1 < nruns ? run_start[r + 1] : npairs;
-  const int per = 32 >> ClassLogL(static_cast<int>(key[run_start[r]] & ((1u << kClassBits) - 1)));
-  run_groups[r] = static_cast<int32_t>((end - run_start[r] + per - 1) / per);
+  const int cls = static_cast<int>(key[run_start[r]] & ((1u << kClassBits) - 1));
+  const int per = 32 >> ClassLogL(cls);
+  int32_t groups = static_cast<int32_t>((end - run_start[r] + per - 1) / per);
+  if (ClassFlat(cls)) {
+    const int q = 8 >> ClassLogB(cls);
+    groups = (groups + q - 1) / q * q;
+  }
+  run_groups[r] = groups;
 }
 
 // Slot of the pair at phase-1 rank i (group * 32 + its place in the group);
@@ -342,7 +359,12 @@ __global__ void iota_kernel(int64_t count, int32_t *out) {
 }
 
 // Entry j (pair k, its e-th id) lands in block e / B of its pair: row
-// (e / B) / L of its group, lane p L + (e / B) % L, position e % B.
+// (e / B) / L of its group, lane p L + (e / B) % L, position e % B.  In a
+// flat run (one block per pair), pair P of the run sits in block P / (32 Q)
+// of 256 ids (Q = 8 / B pairs per 16-byte chunk), chunk P % 32 of it, place
+// (P / 32) % Q in the chunk: lane c of a warp reading chunk c of a block
+// holds pairs c, c + 32, ..., so the warp's stores of the pairs' partials
+// and loads of their dests are lane-consecutive.
 __global__ void scatter_ids_kernel(int64_t m, const int32_t *__restrict__ incl,
                                    const int32_t *__restrict__ pair_pos,
                                    const int32_t *__restrict__ slot_of,
@@ -361,8 +383,16 @@ __global__ void scatter_ids_kernel(int64_t m, const int32_t *__restrict__ incl,
   const int32_t blk = e >> lb;
   const int lane = ((slot & 31) << ll) + (blk & ((1 << ll) - 1));
   const int64_t row = blk >> ll;
-  const int64_t pos = static_cast<int64_t>(rd.z) + static_cast<int64_t>(grp - rd.x) * run_gsize[r] +
-                      ((row * 32 + lane) << lb) + (e & ((1 << lb) - 1));
+  int64_t pos;
+  if (FlatShape(rd.w)) {
+    const int64_t P = static_cast<int64_t>(grp - rd.x) * 32 + (slot & 31);
+    const int64_t in_blk = P % (256 >> lb);
+    pos = static_cast<int64_t>(rd.z) + (P / (256 >> lb)) * 256 + (in_blk & 31) * 8 +
+          ((in_blk >> 5) << lb) + e;
+  } else {
+    pos = static_cast<int64_t>(rd.z) + static_cast<int64_t>(grp - rd.x) * run_gsize[r] +
+          ((row * 32 + lane) << lb) + (e & ((1 << lb) - 1));
+  }
   src[pos] = lid[j];
 }
 
@@ -385,9 +415,6 @@ __global__ void bin_table_kernel(int32_t nbins, const int32_t *__restrict__ bin_
   bin[b] = make_int4(row0, row1, pq[row0], pq[row1]);
 }
 
-// Runs of one block per pair (rows 1, one lane per pair) go to the flat
-// launch of phase 1.
-inline bool FlatShape(int code) { return (code >> 4) == 16; }
 
 // Estimated work of one group of a run (shape code), in thread instructions
 // (the kernels are bound by issue): a flat group is 32 pairs of B ids at
@@ -736,8 +763,8 @@ cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_word
   cub::DoubleBuffer<int32_t> ub(ku[0], ku[1]), pb(kk[0], kk[1]);
   SB_SORT_PAIRS(ub, pb, npairs, 0, BitsFor(ndst));
   const int32_t *u2 = ub.Current(), *k2 = pb.Current();
-  SB_TRY(Keep(sb, &sb->idx, npairs + 8));
-  SB_TRY(cudaMemsetAsync(sb->idx, 0, sizeof(uint16_t) * (npairs + 8), s));
+  SB_TRY(Keep(sb, &sb->idx, npairs + 16));  // read in whole 16-byte words
+  SB_TRY(cudaMemsetAsync(sb->idx, 0, sizeof(uint16_t) * (npairs + 16), s));
   index_kernel<<<Blocks(npairs, T), T, 0, s>>>(npairs, k2, u2, binof, sb->binbase, ppos, sb->idx);
   SB_TRY(Keep(sb, &sb->rowq, ndst + 1));
   SB_TRY(cudaMemcpyAsync(sb->rowq, pq, sizeof(int32_t) * (ndst + 1), cudaMemcpyDeviceToDevice, s));
@@ -765,8 +792,11 @@ cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_word
     for (int64_t r = 0; r < nruns; r++) {
       if (FlatShape(rtab[r].w) != (flat != 0)) continue;
       const int32_t g0 = rgb[r], g1 = rgb[r + 1];
-      const int64_t per = std::max<int64_t>(
+      // flat units hold whole blocks of 8 / B groups
+      const int64_t q = flat ? 8 >> (rtab[r].w & 15) : 1;
+      int64_t per = std::max<int64_t>(
           1, static_cast<int64_t>(target / static_cast<double>(GroupCost(rtab[r].w, flat))));
+      per = (per + q - 1) / q * q;
       for (int64_t g = g0; g < g1; g += per)
         units.push_back(make_int4(static_cast<int32_t>(r), static_cast<int32_t>(g),
                                   static_cast<int32_t>(std::min<int64_t>(g1, g + per)), 0));
