@@ -191,9 +191,11 @@ def measured_peak():
     return HBM_FALLBACK_GBS, "fallback"
 
 
-def profiled_traffic(graph_args: str):
-    """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "pull_sweep_traffic.json")
+def profiled_traffic(graph_args: str, blocked: bool):
+    """DRAM bytes per sweep (all kernels of one sweep) from the committed ncu
+    summary of the sweep layout in use."""
+    name = "blocked_sweep_traffic.json" if blocked else "pull_sweep_traffic.json"
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     with open(p) as fh:
@@ -401,6 +403,9 @@ def run_ours(a, dist: Dist):
     if a.e2e_upload_steps > 0:
         if g is None:
             g = eng.download_graph()  # the generated graph, as a host CSR
+        # a graph solved once per upload: the gather sweep (building the
+        # slice-blocked layout costs more than it saves on one solve)
+        eng.set_sweep_layout("gather")
         per_step, up_sweeps = [], 0
         for i in range(a.e2e_upload_steps + 1):
             torch.cuda.synchronize()
@@ -419,26 +424,48 @@ def run_ours(a, dist: Dist):
         e2e_up = {
             "value": round(dist.sum(float(m) * sweeps_step) / med_s / 1e9, 3), "unit": "GTEPS",
             "h2d_bytes_per_step": 4 * (n + 1) + 4 * m, "d2h_bytes_per_step": 4 * n,
-            "path": "pr_gpu_upload (host CSR, pageable) + pr_gpu_run every step",
+            "path": "pr_gpu_upload (host CSR, pageable) + pr_gpu_run every step, gather sweep "
+                    "layout (one solve per upload)",
             "ms_per_step": round(med_s * 1e3, 3), "statistic": "median step",
             "ms_min": round(dist.max(min(per_step)) * 1e3, 3),
             "ms_max": round(dist.max(max(per_step)) * 1e3, 3),
             "steps": a.e2e_upload_steps,
         }
+        eng.set_sweep_layout("auto")
         eng.set_stream(stream.cuda_stream)
 
-    # ---- roofline of the fused sweep kernel
+    # ---- roofline of the sweep
     peak, peak_src = measured_peak()
     bps = sweep_bytes(n, m, directed)
     avg_sweep_ms = sweep_ms_total / max(sweeps_total, 1)
     achieved = bps / (avg_sweep_ms / 1e3) / 1e9
-    traffic = profiled_traffic(a.graph)
-    # The sweep's gathers (one 4-byte load per edge at a random address) are
-    # bounded by the rate at which L1 misses can be served, measured here on
-    # an L2-resident array: the gather roofline beside the HBM one.
-    from gapbs_b200.pagerank import measure_gather_rate
-    gather_peak = measure_gather_rate(64 << 20, dev)
-    gather_achieved = m / (avg_sweep_ms / 1e3)
+    layout = eng.sweep_layout_info()
+    blocked = layout["last_run_blocked"]
+    traffic = profiled_traffic(a.graph, blocked)
+    # each kernel of the sweep body timed on its own (CUDA events between
+    # separate launches, one extra solve outside the timed region)
+    kms, ksweeps = eng.sweep_kernel_times(a.max_iters, a.epsilon)
+    knames = (["slice_partial_kernel<flat pairs>", "slice_partial_kernel<other pairs>",
+               "bin_row_kernel"] if blocked else ["pull_sweep_kernel"])
+    kernels = [{"kernel": kn, "ms_per_sweep": round(t, 4), "share": round(t / sum(kms), 4)}
+               for kn, t in zip(knames, kms)]
+    if blocked:
+        # bytes the slice-blocked layout moves per sweep: the stored source
+        # ids (2 bytes each, padding included), per (row, slice) pair its
+        # dest (4) and its partial written and read (4 + 4) and its position
+        # in the bin (2); per row its pair range (4), old and new score (8),
+        # next contrib (4) and degree (4); the slices' contribs (4 per vertex)
+        layout_bytes = (2 * layout["ids"] + 14 * layout["pairs"] + 24 * n
+                        + (4 * (n + 1) if directed else 0))
+    else:
+        layout_bytes = bps
+    # The gather sweep's loads (one 4-byte load per edge at a random address)
+    # are bounded by the rate at which L1 misses can be served, measured here
+    # on an L2-resident array: the gather roofline beside the HBM one.
+    if not blocked:
+        from gapbs_b200.pagerank import measure_gather_rate
+        gather_peak = measure_gather_rate(64 << 20, dev)
+        gather_achieved = m / (avg_sweep_ms / 1e3)
 
     result = {
         "metric": METRIC,
@@ -456,6 +483,10 @@ def run_ours(a, dist: Dist):
         "config": {
             "workload": f"PageRankPull {a.graph.strip()} (Kronecker/uniform per pr_spmv options), "
                         f"damping 0.85, epsilon {a.epsilon}, max_iters {a.max_iters}",
+            "sweep_layout": ({"layout": "slice-blocked", "slices": layout["slices"],
+                              "bins": layout["bins"], "pairs": layout["pairs"],
+                              "stored_ids": layout["ids"], "device_bytes": layout["bytes"]}
+                             if blocked else {"layout": "gather"}),
             "num_nodes": n, "num_edges_directed": m, "sweeps_per_step": sweeps_per_step,
             "l2": "256 MB buffer written between steps; graph 4M+4N bytes >> 126 MB L2",
             "parallelism": f"replicas{dist.world}" if dist.world > 1 else "single GPU",
@@ -472,7 +503,8 @@ def run_ours(a, dist: Dist):
             "ms_per_step": round(e2e_s * 1e3 / a.steps, 4),
         },
         "roofline": {
-            "kernel": "pull_sweep_kernel",
+            "kernel": ("slice-blocked sweep: " + ", ".join(knames) + " (one launch each per "
+                       "sweep)") if blocked else "pull_sweep_kernel",
             "bound": "hbm",
             "achieved": round(achieved, 1),
             "peak": peak,
@@ -482,18 +514,27 @@ def run_ours(a, dist: Dist):
             "traffic": traffic,
             "algorithmic_bytes_per_sweep": bps,
             "avg_sweep_ms": round(avg_sweep_ms, 4),
-            "gather": {
-                "achieved": round(gather_achieved / 1e9, 2),
-                "peak": round(gather_peak / 1e9, 2),
-                "unit": "G gathers/s",
-                "frac": round(gather_achieved / gather_peak, 4),
-                "peak_source": "measured in this run: random 4-byte loads (ld.global.nc) "
-                               "from a 64 MB L2-resident array",
-            },
+            "kernels": kernels,
+            "kernels_note": "average device ms per sweep of each kernel, each launched on its "
+                            f"own between CUDA events ({ksweeps} sweeps, one solve outside the "
+                            "timed region)",
+            "layout_bytes_per_sweep": int(layout_bytes),
+            "layout_gbs": round(layout_bytes / (avg_sweep_ms / 1e3) / 1e9, 1),
+            "layout_frac": round(layout_bytes / (avg_sweep_ms / 1e3) / 1e9 / peak, 4),
         },
         "clocks": clk,
         "gpu_launches": int(launches),
     }
+    if not blocked:
+        # the gather sweep's ceiling: one random 4-byte load per edge
+        result["roofline"]["gather"] = {
+            "achieved": round(gather_achieved / 1e9, 2),
+            "peak": round(gather_peak / 1e9, 2),
+            "unit": "G gathers/s",
+            "frac": round(gather_achieved / gather_peak, 4),
+            "peak_source": "measured in this run: random 4-byte loads (ld.global.nc) "
+                           "from a 64 MB L2-resident array",
+        }
     if e2e_up is not None:
         result["e2e_graph_upload_each_step"] = e2e_up
     if cc is not None:
@@ -512,7 +553,7 @@ def run_ours(a, dist: Dist):
     if not a.no_cpu_baseline and dist.rank == 0 and dist.world == 1:
         if g is None:
             g = eng.download_graph()  # the generated graph, for the reference on the host
-        result["cpu_baseline"] = cpu_baseline(g, a, sweeps_per_step)
+        result["cpu_baseline"] = cpu_baseline(g, a, sweeps_per_step, max_ms / a.steps)
         if bfs is not None and bfs["sources"]:
             import oracle
             if oracle.ref_available():
@@ -613,9 +654,9 @@ def run_ppr(a, dev):
                                       "loads) from a 64 MB L2-resident array",
                        "peak_1gb_array": round(row_peak_hbm, 1),
                        "frac_1gb_array": round(gathered_gbs / row_peak_hbm, 4)},
-            "note": "hub rows hit L2, the rest come from HBM (63 % L2 hit at g22, profiles/"
-                    "batch_sweep_g22_metrics.md): the rate lies between the L2-resident "
-                    "and the 1 GB-array row-gather ceilings",
+            "note": "hub rows hit L2, the rest come from HBM (63 % L2 hit at g22 by ncu): "
+                    "the rate lies between the L2-resident and the 1 GB-array row-gather "
+                    "ceilings",
         },
         "batched_gteps": round(b_gteps, 3),
         "batched_ms": round(b_ms, 3),
@@ -665,6 +706,38 @@ def run_adjoint(a, dev):
     f_ms, a_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
     eng.close()
     asw = int(asw)
+    # a training loop through torch.autograd: forward, backward, SGD step on
+    # the edge weights; the graph is uploaded once, each later step hands
+    # the new weights to the engine from device memory
+    from gapbs_b200.autograd import PageRankContext, personalized_pagerank
+    pctx = PageRankContext(g, device=dev, max_iters=100, epsilon=1e-7, adjoint_max_iters=300,
+                           adjoint_epsilon=1e-7)
+    wt = torch.tensor(ew, device=f"cuda:{dev}", requires_grad=True)
+
+    def train_step():
+        sp = personalized_pagerank(t, wt, pctx)
+        loss = (w * sp).sum()
+        wt.grad = None
+        loss.backward()
+        with torch.no_grad():
+            wt.sub_(1e3 * wt.grad)
+            wt.clamp_(min=0.05)
+
+    train_step()  # warm-up: the one graph upload
+    torch.cuda.synchronize()
+    steps = 10
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        train_step()
+    torch.cuda.synchronize()
+    train_ms = (time.perf_counter() - t0) * 1e3 / steps
+    train = {"steps": steps, "ms_per_step": round(train_ms, 3),
+             "graph_uploads_in_timed_steps": pctx.uploads - 1,
+             "device_weight_updates_in_timed_steps": pctx.weight_updates,
+             "host_device_graph_bytes_per_step": 0,
+             "path": "torch.autograd (personalized_pagerank) forward + backward + SGD on edge "
+                     "weights; pr_gpu_set_edge_weights_device each step"}
+    pctx.engine.close()
     # adjoint sweeps read ids, weights and offsets of the out-rows (8M + 4(N+1))
     # plus 16N of vectors; the gradient pass reads 8M and writes 4M
     adj_bytes = asw * (8.0 * m + 4.0 * (n + 1) + 16.0 * n) + 12.0 * m
@@ -673,12 +746,13 @@ def run_adjoint(a, dev):
                     f"U[0.5,1.5], loss weights N(0,1), epsilon 1e-7",
         "forward_sweeps": int(fsw[0]), "forward_ms": round(f_ms, 3),
         "adjoint_sweeps": asw, "adjoint_ms": round(a_ms, 3),
+        "autograd_training": train,
         "adjoint_gteps": round(m * asw / (a_ms / 1e3) / 1e9, 2),
         "adjoint_algorithmic_gbs": round(adj_bytes / (a_ms / 1e3) / 1e9, 1),
     }
 
 
-def cpu_baseline(g, a, gpu_sweeps):
+def cpu_baseline(g, a, gpu_sweeps, gpu_ms_per_solve):
     import oracle
     cores = os.cpu_count() or 1
     n, m = g.num_nodes, g.num_edges_directed
@@ -688,11 +762,27 @@ def cpu_baseline(g, a, gpu_sweeps):
                                          epsilon=a.epsilon)
         sweeps = gpu_sweeps
         sec = float(np.mean(per))
+        # the reference's pr benchmark: Gauss-Seidel PageRankPullGS on the
+        # same graph (its own convergence test, fewer sweeps), for time to
+        # solution
+        _, log = capture_fd1(rg.pagerank_gs, a.max_iters, a.epsilon, True)
+        gs_sweeps = len([ln for ln in log.splitlines() if ln.strip()])
+        _, gper = rg.time_pagerank_gs(trials=a.cpu_trials, max_iters=a.max_iters,
+                                      epsilon=a.epsilon)
+        gsec = float(np.mean(gper))
         return {"value": round(m * sweeps / sec / 1e9, 4), "unit": "GTEPS", "cores": cores,
                 "kind": "reference",
                 "sample": f"{a.cpu_trials} full PageRankPull solves of the same graph "
                           f"({sweeps:.0f} sweeps each) by the reference compiled from source, "
-                          f"OpenMP on {cores} threads; {sec:.3f} s per solve"}
+                          f"OpenMP on {cores} threads; {sec:.3f} s per solve",
+                "gauss_seidel": {
+                    "kernel": "PageRankPullGS (src/pr.cc:34-61), the reference's pr benchmark",
+                    "value": round(m * gs_sweeps / gsec / 1e9, 4), "unit": "GTEPS",
+                    "sweeps": gs_sweeps, "s_per_solve": round(gsec, 4), "cores": cores,
+                    "sample": f"{a.cpu_trials} full solves of the same graph, OpenMP on "
+                              f"{cores} threads",
+                    "gpu_speedup_time_to_solution": round(gsec * 1e3 / gpu_ms_per_solve, 2),
+                }}
     # port: single-threaded FP32 oracle, 2 sweeps
     t0 = time.perf_counter()
     _, k, _ = oracle.pr_pull_f32(g, max_iters=2, epsilon=0.0)

@@ -8,8 +8,9 @@ GPU engine, and its backward pass runs the engine's adjoint:
     dL/dt         = (1-d) lambda
     dL/dw(v->u)   = d s[v] / S_v (lambda[u] - (P lambda)[v])
 with edge_w aligned with the graph's out-CSR.  All tensors live on the
-engine's CUDA device (float32); no host round trips except a re-upload when
-the edge weights change.
+engine's CUDA device (float32).  The graph is uploaded once; new edge
+weights (a training step) go to the engine from device memory
+(pr_gpu_set_edge_weights_device), with no host round trip.
 """
 from __future__ import annotations
 
@@ -37,16 +38,31 @@ class PageRankContext:
     _weights_key: Optional[tuple] = field(default=None, init=False)
     last_sweeps: int = field(default=0, init=False)
     last_adjoint_sweeps: int = field(default=0, init=False)
+    uploads: int = field(default=0, init=False)          # full graph uploads
+    weight_updates: int = field(default=0, init=False)   # device weight updates
 
     def __post_init__(self):
         self.engine = PageRankEngine(self.device)
 
     def ensure_weights(self, edge_w: Optional[torch.Tensor]):
+        """Puts edge_w (or unit weights for None) in the engine: a full
+        upload the first time and when switching between weighted and
+        unweighted, else a device-to-device weight update."""
         key = None if edge_w is None else (edge_w.data_ptr(), edge_w._version, edge_w.numel())
         if self._weights_key is not None and key == self._weights_key[0]:
             return
-        w = None if edge_w is None else edge_w.detach().float().cpu().numpy()
-        self.engine.upload(self.graph, edge_w=w)
+        was_weighted = self._weights_key is not None and self._weights_key[0] is not None
+        if edge_w is not None and was_weighted:
+            if edge_w.numel() != self.engine.m:
+                raise ValueError("edge_w must have one entry per directed edge")
+            w = _cuda_f32(edge_w, self.device)
+            torch.cuda.current_stream(w.device).synchronize()
+            self.engine.set_edge_weights_device(w.data_ptr())
+            self.weight_updates += 1
+        else:
+            w = None if edge_w is None else edge_w.detach().float().cpu().numpy()
+            self.engine.upload(self.graph, edge_w=w)
+            self.uploads += 1
         self._weights_key = (key,)
 
 

@@ -270,11 +270,10 @@ slice_partial_kernel(const BlockedArgs a) {
 
 // Phase 2: one CTA per bin of rows (then blocks for the rows without
 // in-edges, on the first sweep only).  The bin's partials, one contiguous
-// block of part[], are copied into shared memory (blk); the bin's stretch
-// of idx[] (its pairs in row order, each a position in the block) is
-// streamed with coalesced 16-byte loads and turned into the partials in row
-// order (ord); then each thread takes rows u = row0 + t, + kBinThreads, ...
-// and sums the row's stretch of ord in slice order.
+// block of part[], are copied into shared memory; then each thread takes
+// rows u = row0 + t, + kBinThreads, ...: it sums the row's partials in slice
+// order (their positions in the block: idx[rowq[u] .. rowq[u + 1])) and
+// updates the row.
 __global__ void __launch_bounds__(kBinThreads)
 bin_row_kernel(const BlockedArgs a) {
   if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
@@ -291,71 +290,39 @@ bin_row_kernel(const BlockedArgs a) {
   if (b < a.nbins) {
     const int4 bn = a.bin[b];
     const int row0 = bn.x, row1 = bn.y, q0 = bn.z, q1 = bn.w;
-    const int np = q1 - q0;
-    const int np4 = (np + 3) >> 2;  // the block is padded to whole float4
-    float *blk = sm;                // the bin's partials, block order
-    float *ord = sm + 4 * np4;      // the same, in (row, slice) order (16-byte aligned)
+    const int np4 = (q1 - q0 + 3) >> 2;  // the block is padded to whole float4
     const float4 *src4 = reinterpret_cast<const float4 *>(a.part + a.binbase[b]);
-    float4 *blk4 = reinterpret_cast<float4 *>(blk);
-    for (int i = threadIdx.x; i < np4; i += kBinThreads) cp_async_16(blk4 + i, src4 + i);
+    float4 *sm4 = reinterpret_cast<float4 *>(sm);
+    for (int i = threadIdx.x; i < np4; i += kBinThreads) cp_async_16(sm4 + i, src4 + i);
     // the first row's own data is fetched while the block arrives
     int u = row0 + threadIdx.x;
     int s0 = 0, s1 = 0;
     float old = 0.f;
     if (u < row1) {
-      s0 = a.rowq[u] - q0;
-      s1 = a.rowq[u + 1] - q0;
+      s0 = a.rowq[u];
+      s1 = a.rowq[u + 1];
       old = ld_score(a.score + u, ps);
-    }
-    // idx[q0 .. q1): 8 positions per 16-byte load; the stretch's first and
-    // last loads are masked to it
-    const int e0 = q0 & ~7, e1 = (q1 + 7) & ~7;
-    const int nq = (e1 - e0) >> 3;
-    uint4 iq[4];
-    const uint4 *idx4 = reinterpret_cast<const uint4 *>(a.idx + e0);
-#pragma unroll
-    for (int t = 0; t < 4; t++) {
-      const int c = threadIdx.x + t * kBinThreads;
-      if (c < nq) iq[t] = ld_stream_u4(idx4 + c, ps);
     }
     cp_async_wait_all();
     __syncthreads();
-    const unsigned blkb = smem_addr(blk);
-    // ord[j - e0] holds pair j's partial: each thread writes its 8 as two
-    // aligned 16-byte stores (entries outside [q0, q1) get a zero)
-    for (int c0 = 0; c0 < nq; c0 += 4 * kBinThreads) {
-#pragma unroll
-      for (int t = 0; t < 4; t++) {
-        const int c = c0 + threadIdx.x + t * kBinThreads;
-        if (c >= nq) break;
-        const unsigned w[4] = {iq[t].x, iq[t].y, iq[t].z, iq[t].w};
-        float v[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const int j = e0 + c * 8 + k;  // pair number in the stream
-          v[k] = (j >= q0 && j < q1)
-                     ? lds_f32(blkb, (k & 1) ? (w[k >> 1] >> 16) : (w[k >> 1] & 0xffffu))
-                     : 0.f;
-        }
-        float4 *o4 = reinterpret_cast<float4 *>(ord) + 2 * c;
-        o4[0] = make_float4(v[0], v[1], v[2], v[3]);
-        o4[1] = make_float4(v[4], v[5], v[6], v[7]);
-        const int cn = c + 4 * kBinThreads;
-        if (cn < nq) iq[t] = ld_stream_u4(idx4 + cn, ps);
-      }
-    }
-    __syncthreads();
-    const unsigned ordb = smem_addr(ord) + 4u * static_cast<unsigned>(q0 - e0);
+    const unsigned smb = smem_addr(sm);
     while (u < row1) {
       float sum = 0.f;
-#pragma unroll 4
-      for (int j = s0; j < s1; j++) sum = __fadd_rn(sum, lds_f32(ordb, j));
+      int j = s0;
+      for (; j + 3 < s1; j += 4) {
+        const unsigned i0 = a.idx[j], i1 = a.idx[j + 1], i2 = a.idx[j + 2], i3 = a.idx[j + 3];
+        sum = __fadd_rn(sum, lds_f32(smb, i0));
+        sum = __fadd_rn(sum, lds_f32(smb, i1));
+        sum = __fadd_rn(sum, lds_f32(smb, i2));
+        sum = __fadd_rn(sum, lds_f32(smb, i3));
+      }
+      for (; j < s1; j++) sum = __fadd_rn(sum, lds_f32(smb, a.idx[j]));
       const int un = u + kBinThreads;
       int n0 = 0, n1 = 0;
       float nold = 0.f;
       if (un < row1) {  // the next row's data, fetched before this row is written
-        n0 = a.rowq[un] - q0;
-        n1 = a.rowq[un + 1] - q0;
+        n0 = a.rowq[un];
+        n1 = a.rowq[un + 1];
         nold = ld_score(a.score + un, ps);
       }
       const float base = a.kind == kKindPPR ? a.base_vec[u] : a.base_scalar;
@@ -403,7 +370,6 @@ int BinRowGrid(const SliceBlocks &sb, int64_t n) {
 
 // contribs + the zero slot, rounded to whole float4
 size_t SliceSmemBytes(const SliceBlocks &sb) { return sizeof(float) * (sb.slice_verts + 4); }
-// the bin's partials twice (block order; row order from a multiple of 8)
-size_t BinSmemBytes(const SliceBlocks &sb) { return sizeof(float) * (2 * sb.bin_words + 16); }
+size_t BinSmemBytes(const SliceBlocks &sb) { return sizeof(float) * sb.bin_words; }
 
 }  // namespace prgpu

@@ -48,10 +48,10 @@ namespace prgpu {
 constexpr int kSliceWarps = 32;
 constexpr int kBinWarps = 8;
 constexpr int kDefaultSliceVerts = 49152;  // 192 KB of contribs in shared memory
-constexpr int kDefaultBinWords = 6144;     // partials per bin (pairs + rows): 2 x 24 KB of shared memory
+constexpr int kDefaultBinWords = 6144;     // 24 KB of partials per bin (pairs + rows)
 constexpr int kMaxSliceVerts = 56320;      // + the zero slot, within one CTA's shared memory
 constexpr int kMaxPairIds = 2048;          // longer (row, slice) pairs are cut into pieces
-constexpr int kMaxBinWords = 28160;        // two copies of a bin's partials in shared memory
+constexpr int kMaxBinWords = 28160;
 struct SliceBlocks {
   bool ready = false;
   int32_t slice_verts = 0;   // source ids per slice
@@ -87,9 +87,11 @@ struct SliceBlocks {
 
 // Builds the layout from the renumbered in-CSR of g (unweighted).  Leaves
 // sb->ready false (and returns cudaSuccess) when the graph does not fit the
-// layout's limits.  slice_verts / bin_words: 0 for the defaults.
+// layout's limits or has more than max_pairs (row, slice) pairs.
+// slice_verts / bin_words: 0 for the defaults.
 cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_words,
-                             SliceBlocks *sb, cudaStream_t s, std::string *err);
+                             int64_t max_pairs, SliceBlocks *sb, cudaStream_t s,
+                             std::string *err);
 void FreeSliceBlocks(SliceBlocks *sb);
 
 // Kernel-side view of one sweep of the slice-blocked path.

@@ -528,7 +528,8 @@ void FreeSliceBlocks(SliceBlocks *sb) {
   } while (0)
 
 cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_words,
-                             SliceBlocks *sb, cudaStream_t s, std::string *err) {
+                             int64_t max_pairs, SliceBlocks *sb, cudaStream_t s,
+                             std::string *err) {
   FreeSliceBlocks(sb);
   if (slice_verts <= 0) slice_verts = kDefaultSliceVerts;
   if (bin_words <= 0) bin_words = kDefaultBinWords;
@@ -600,6 +601,7 @@ cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_word
   int32_t npairs = 0;
   SB_TRY(cudaMemcpyAsync(&npairs, incl + (m - 1), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   SB_TRY(cudaStreamSynchronize(s));
+  if (npairs > max_pairs) return cudaSuccess;  // the caller keeps the gather sweep
   int32_t *pair_u = nullptr, *pair_c = nullptr, *pair_pos = nullptr, *pair_len = nullptr;
   SB_TRY(tmp.Get(&pair_u, npairs));
   SB_TRY(tmp.Get(&pair_c, npairs));

@@ -52,6 +52,8 @@ struct DeviceGraph {
   int32_t *rowoff = nullptr;   // n+1
   int32_t *col = nullptr;      // m rounded up to a multiple of 4
   float *win = nullptr;        // weighted: w(v->u) aligned with col
+  int32_t *win_pos = nullptr;  // weighted: where each win entry's weight sits in
+                               // the caller's out-CSR (for weight updates)
   // out-direction data in new ids
   int32_t *odeg = nullptr;     // directed: out-degree per new id
   float *rsum = nullptr;       // weighted: S_v = sum of out-weights per new id
@@ -158,6 +160,12 @@ cudaError_t BuildDeviceGraph(DeviceGraph *g, int64_t n, int64_t m,
                              const float *d_ew, bool directed,
                              cudaStream_t s, std::string *err);
 void FreeDeviceGraph(DeviceGraph *g);
+// New edge weights for a weighted graph already on the device: d_w holds one
+// weight per entry of the caller's out-CSR (as uploaded).  Checked first
+// (finite and positive, else cudaErrorInvalidValue and the old weights stay),
+// then rsum, win and wout are rebuilt on the device.
+cudaError_t UpdateDeviceWeights(DeviceGraph *g, const float *d_w, cudaStream_t s,
+                                std::string *err);
 
 // The reference's -g / -u graph built on the device (generate.cu): CSR of
 // the symmetrised, squished graph in original ids, int32 offsets (n+1) and

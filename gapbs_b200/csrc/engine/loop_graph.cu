@@ -157,6 +157,27 @@ cudaError_t LoopGraph::Launch(const SweepKernel *ks, int nk, LoopCtl *ctl, int m
   return cudaGraphLaunch(exec_, s);
 }
 
+cudaError_t LoopGraph::LaunchTimed(const SweepKernel *ks, int nk, LoopCtl *ctl, int max_iters,
+                                   cudaStream_t s, const cudaEvent_t *ev) {
+  std::vector<std::vector<unsigned char>> blobs;
+  for (int k = 0; k < nk; k++)
+    blobs.emplace_back(static_cast<const unsigned char *>(ks[k].args),
+                       static_cast<const unsigned char *>(ks[k].args) + ks[k].args_size);
+  for (int i = 0; i < max_iters; i++) {
+    for (int k = 0; k < nk; k++) {
+      cudaError_t e = cudaEventRecord(ev[i * (nk + 1) + k], s);
+      if (e != cudaSuccess) return e;
+      void *params[] = {blobs[k].data()};
+      e = cudaLaunchKernel(ks[k].fn, ks[k].grid, ks[k].block, params, ks[k].smem, s);
+      if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = cudaEventRecord(ev[i * (nk + 1) + nk], s);
+    if (e != cudaSuccess) return e;
+    loop_advance_kernel<<<1, 32, 0, s>>>(ctl, max_iters);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t LoopGraph::Launch(const void *fn, dim3 grid, dim3 block, const void *args,
                               size_t args_size, LoopCtl *ctl, int max_iters, cudaStream_t s) {
   SweepKernel k;

@@ -57,6 +57,12 @@ class LoopGraph {
   cudaError_t Launch(const SweepKernel *ks, int nk, LoopCtl *ctl, int max_iters,
                      cudaStream_t s);
   void Reset();
+  // Measurement: the same sweeps as Launch(ks, nk, ...) issued as ordinary
+  // launches, with ev[i (nk + 1) + k] recorded before kernel k of sweep i
+  // and ev[i (nk + 1) + nk] after its last kernel (max_iters (nk + 1)
+  // events).  Sweeps after the loop stopped return at once.
+  static cudaError_t LaunchTimed(const SweepKernel *ks, int nk, LoopCtl *ctl, int max_iters,
+                                 cudaStream_t s, const cudaEvent_t *ev);
 
  private:
   cudaError_t Build(const SweepKernel *ks, int nk, LoopCtl *ctl, int max_iters);

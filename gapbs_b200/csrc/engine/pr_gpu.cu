@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <new>
 #include <string>
@@ -45,6 +46,12 @@ struct pr_gpu {
   int64_t last_launches = 0;
   int last_adjoint_sweeps = 0;
   bool last_blocked = false;
+  // pr_gpu_sweep_kernel_times: per-kernel events of one timed solve and the
+  // average device ms per sweep of each kernel of the sweep body
+  bool time_kernels = false;
+  std::vector<cudaEvent_t> kev;
+  double kernel_ms[3] = {0, 0, 0};
+  int kernel_n = 0;
   // pinned staging for host <-> device copies
   static constexpr size_t kChunk = 32u << 20;
   void *pinned[2] = {nullptr, nullptr};
@@ -309,14 +316,20 @@ int CheckRunArgs(pr_gpu_t *h, int max_iters, int ncols) {
 
 // Builds the slice-blocked layout of the current graph when the layout
 // setting asks for it.  Under PR_GPU_SWEEP_AUTO a graph outside the layout's
-// limits, or a device without room for it, keeps the gather sweep.
+// limits, a device without room for it, or a graph whose in-edges hardly
+// share (row, slice) pairs (more pairs than half the edges: one partial
+// written and read per edge costs more than the gather it replaces, as on
+// uniform random graphs) keeps the gather sweep.
 int EnsureSliceBlocks(pr_gpu_t *h) {
   if (h->sb_built || h->sweep_layout == PR_GPU_SWEEP_GATHER || !h->has_graph) return PR_GPU_OK;
   h->sb_built = true;
   h->loop_blocked.Reset();
   std::string msg;
-  cudaError_t e = prgpu::BuildSliceBlocks(h->g, h->slice_verts, h->bin_words, &h->sb, h->stream,
-                                          &msg);
+  const int64_t max_pairs = h->sweep_layout == PR_GPU_SWEEP_AUTO
+                                ? h->g.m / 2
+                                : std::numeric_limits<int64_t>::max();
+  cudaError_t e = prgpu::BuildSliceBlocks(h->g, h->slice_verts, h->bin_words, max_pairs, &h->sb,
+                                          h->stream, &msg);
   if (e == cudaSuccess) return PR_GPU_OK;
   cudaGetLastError();
   if (h->sweep_layout == PR_GPU_SWEEP_AUTO && e == cudaErrorMemoryAllocation) return PR_GPU_OK;
@@ -464,7 +477,25 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
     }
   }
   PR_CHECK(h, cudaEventRecord(h->ev[1], s));
-  if (blocked)
+  prgpu::SweepKernel gather_body;
+  gather_body.fn = sweep_fn;
+  gather_body.grid = dim3(nblocks);
+  gather_body.block = dim3(prgpu::kSweepThreads);
+  gather_body.args = &a;
+  gather_body.args_size = sizeof(a);
+  const prgpu::SweepKernel *tk = blocked ? body : &gather_body;
+  const int tnk = blocked ? 3 : 1;
+  const bool timed = h->time_kernels && max_iters > 0 && (blocked || nblocks > 0);
+  if (timed) {
+    const size_t need = static_cast<size_t>(max_iters) * (tnk + 1);
+    while (h->kev.size() < need) {
+      cudaEvent_t e = nullptr;
+      PR_CHECK(h, cudaEventCreate(&e));
+      h->kev.push_back(e);
+    }
+    PR_CHECK(h, prgpu::LoopGraph::LaunchTimed(tk, tnk, &sc.ctl->loop, max_iters, s,
+                                              h->kev.data()));
+  } else if (blocked)
     PR_CHECK(h, h->loop_blocked.Launch(body, 3, &sc.ctl->loop, max_iters, s));
   else if (nblocks > 0)
     PR_CHECK(h, h->loop_single.Launch(sweep_fn, dim3(nblocks),
@@ -486,6 +517,21 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
   cudaEventElapsedTime(&ms_total, h->ev[0], h->ev[3]);
   h->last_sweep_ms = ms_sweep;
   h->last_total_ms = ms_total;
+  if (timed) {
+    // the sweeps that ran: every one counted by the loop, none after it
+    const int ran = std::min(ctl.loop.loops, max_iters);
+    h->kernel_n = tnk;
+    for (int k = 0; k < tnk; k++) {
+      double sum = 0;
+      for (int i = 0; i < ran; i++) {
+        float t = 0;
+        PR_CHECK(h, cudaEventElapsedTime(&t, h->kev[i * (tnk + 1) + k],
+                                         h->kev[i * (tnk + 1) + k + 1]));
+        sum += t;
+      }
+      h->kernel_ms[k] = ran ? sum / ran : 0.0;
+    }
+  }
   // per sweep: the sweep kernel(s) + the decide kernel
   h->last_launches = launches + (blocked ? 4 : 2) * static_cast<int64_t>(ctl.loop.loops);
   h->last_blocked = blocked;
@@ -622,6 +668,8 @@ void pr_gpu_destroy(pr_gpu_t *h) {
     if (h->pin_ev[i]) cudaEventDestroy(h->pin_ev[i]);
   }
   for (auto &e : h->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto &e : h->kev)
     if (e) cudaEventDestroy(e);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
@@ -914,6 +962,23 @@ int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m, const int32_t *out_off,
   return EnsureSliceBlocks(h);
 }
 
+int pr_gpu_set_edge_weights_device(pr_gpu_t *h, const float *w_dev) {
+  if (!h) return PR_GPU_EINVAL;
+  if (!h->has_graph) return SetErr(h, PR_GPU_ENOGRAPH, "no graph uploaded");
+  if (!h->g.weighted)
+    return SetErr(h, PR_GPU_EINVAL, "the uploaded graph has no edge weights");
+  if (!w_dev && h->g.m) return SetErr(h, PR_GPU_EINVAL, "w_dev is null");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  std::string msg;
+  cudaError_t e = prgpu::UpdateDeviceWeights(&h->g, w_dev, h->stream, &msg);
+  if (e == cudaErrorInvalidValue && msg.rfind("invalid edge weights", 0) == 0)
+    return SetErr(h, PR_GPU_EGRAPH, msg);
+  if (e != cudaSuccess)
+    return SetErr(h, e == cudaErrorMemoryAllocation ? PR_GPU_ENOMEM : PR_GPU_ECUDA,
+                  msg.empty() ? std::string(cudaGetErrorString(e)) : msg);
+  return PR_GPU_OK;
+}
+
 int pr_gpu_run_device(pr_gpu_t *h, int max_iters, double epsilon, float damping, int ncols,
                       const float *teleport_dev, float *scores_out_dev, int32_t *sweeps_out,
                       double *err_trace) {
@@ -1053,6 +1118,24 @@ int pr_gpu_sweep_layout_info(pr_gpu_t *h, int *blocked, int *slices, int *bins, 
   if (ids) *ids = on ? h->sb.elems : 0;
   if (bytes) *bytes = on ? static_cast<int64_t>(h->sb.bytes) : 0;
   if (last_blocked) *last_blocked = h->last_blocked ? 1 : 0;
+  return PR_GPU_OK;
+}
+
+int pr_gpu_sweep_kernel_times(pr_gpu_t *h, int max_iters, double epsilon, double *ms,
+                              int max_kernels, int *nkernels, int32_t *sweeps_out) {
+  int rc = CheckRunArgs(h, max_iters, 1);
+  if (rc) return rc;
+  if (!ms || max_kernels < 3) return SetErr(h, PR_GPU_EINVAL, "ms is null or max_kernels < 3");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  rc = EnsureScratch(h, h->g.n, 1, 1, std::max(max_iters, 1));
+  if (rc) return rc;
+  h->time_kernels = true;
+  h->kernel_n = 0;
+  rc = SolveSingle(h, max_iters, epsilon, 0.85f, nullptr, h->sc.outbuf, sweeps_out, nullptr);
+  h->time_kernels = false;
+  if (rc) return rc;
+  for (int k = 0; k < h->kernel_n; k++) ms[k] = h->kernel_ms[k];
+  if (nkernels) *nkernels = h->kernel_n;
   return PR_GPU_OK;
 }
 

@@ -144,7 +144,7 @@ __global__ void in_weight_kernel(int64_t n, const int32_t *__restrict__ perm,
                                  const int32_t *__restrict__ out_nbr,
                                  const float *__restrict__ ew,
                                  const int32_t *__restrict__ rowoff, float *win,
-                                 unsigned *flag) {
+                                 int32_t *win_pos, unsigned *flag) {
   const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
@@ -160,8 +160,10 @@ __global__ void in_weight_kernel(int64_t n, const int32_t *__restrict__ perm,
     }
     if (lo < out_off[x + 1] && out_nbr[lo] == v) {
       win[d + j] = ew[lo];
+      win_pos[d + j] = lo;
     } else {
       win[d + j] = 0.f;
+      win_pos[d + j] = -1;
       atomicOr(flag, kBadOffsetOrder);  // in/out CSRs disagree
     }
   }
@@ -189,6 +191,15 @@ inline unsigned Blocks(int64_t count, int threads) {
   return static_cast<unsigned>((count + threads - 1) / threads);
 }
 
+// win[j] = w[win_pos[j]] over the renumbered in-CSR entries.
+__global__ void gather_weights_kernel(int64_t m, const int32_t *__restrict__ pos,
+                                      const float *__restrict__ w, float *out) {
+  const int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const int32_t p = pos[j];
+  out[j] = p >= 0 ? w[p] : 0.f;
+}
+
 std::string FlagText(unsigned f) {
   std::string s;
   if (f & kBadOffsetStart) s += " offsets[0] != 0;";
@@ -210,8 +221,8 @@ cudaError_t Alloc(T **p, int64_t count) {
 }  // namespace
 
 void FreeDeviceGraph(DeviceGraph *g) {
-  void *ptrs[] = {g->rowoff, g->col, g->win, g->odeg, g->rsum, g->orowoff, g->ocol, g->wout,
-                  g->orig_out_off, g->perm, g->inv, g->seg_row, g->seg_first, g->hub_ticket,
+  void *ptrs[] = {g->rowoff, g->col, g->win, g->win_pos, g->odeg, g->rsum, g->orowoff, g->ocol,
+                  g->wout, g->orig_out_off, g->perm, g->inv, g->seg_row, g->seg_first, g->hub_ticket,
                   g->seg_partial};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -336,8 +347,10 @@ cudaError_t BuildDeviceGraph(DeviceGraph *g, int64_t n, int64_t m,
     row_weight_sum_kernel<<<Blocks(n, T), T, 0, s>>>(n, g->perm, d_out_off, d_ew, g->rsum);
     PR_TRY(Alloc(&g->win, m_pad));
     PR_TRY(cudaMemsetAsync(g->win, 0, sizeof(float) * m_pad, s));
+    PR_TRY(Alloc(&g->win_pos, m_pad));
     in_weight_kernel<<<Blocks(n * 32, T), T, 0, s>>>(n, g->perm, d_in_off, d_in_nbr, d_out_off,
-                                                     d_out_nbr, d_ew, g->rowoff, g->win, d_flag);
+                                                     d_out_nbr, d_ew, g->rowoff, g->win,
+                                                     g->win_pos, d_flag);
     const int32_t *oro = directed ? g->orowoff : g->rowoff;
     PR_TRY(Alloc(&g->wout, m_pad));
     PR_TRY(cudaMemsetAsync(g->wout, 0, sizeof(float) * m_pad, s));
@@ -389,6 +402,43 @@ cudaError_t BuildDeviceGraph(DeviceGraph *g, int64_t n, int64_t m,
   if (nseg)
     PR_TRY(cudaMemcpy(g->seg_row, seg_row.data(), sizeof(int32_t) * nseg, cudaMemcpyHostToDevice));
   PR_TRY(cudaMemsetAsync(g->hub_ticket, 0, sizeof(unsigned) * std::max<int64_t>(H, 1), s));
+  PR_TRY(cudaStreamSynchronize(s));
+  cleanup();
+  return cudaSuccess;
+}
+
+cudaError_t UpdateDeviceWeights(DeviceGraph *g, const float *d_w, cudaStream_t s,
+                                std::string *err) {
+  if (!g->weighted || !g->win_pos) {
+    *err = "the graph on the device has no edge weights";
+    return cudaErrorInvalidValue;
+  }
+  const int64_t n = g->n, m = g->m;
+  const int T = 256;
+  unsigned *d_flag = nullptr;
+  auto cleanup = [&]() {
+    if (d_flag) cudaFree(d_flag);
+    d_flag = nullptr;
+  };
+  PR_TRY(Alloc(&d_flag, 1));
+  PR_TRY(cudaMemsetAsync(d_flag, 0, sizeof(unsigned), s));
+  if (m) validate_weights_kernel<<<Blocks(m, T), T, 0, s>>>(m, d_w, d_flag);
+  PR_TRY(cudaGetLastError());
+  unsigned flag = 0;
+  PR_TRY(cudaMemcpyAsync(&flag, d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  PR_TRY(cudaStreamSynchronize(s));
+  if (flag) {
+    *err = "invalid edge weights:" + FlagText(flag);
+    cleanup();
+    return cudaErrorInvalidValue;
+  }
+  // the same three arrays BuildDeviceGraph derives from the weights
+  row_weight_sum_kernel<<<Blocks(n, T), T, 0, s>>>(n, g->perm, g->orig_out_off, d_w, g->rsum);
+  if (m) gather_weights_kernel<<<Blocks(m, T), T, 0, s>>>(m, g->win_pos, d_w, g->win);
+  const int32_t *oro = g->directed ? g->orowoff : g->rowoff;
+  renumber_rows_kernel<<<Blocks(n * 32, T), T, 0, s>>>(n, g->perm, g->orig_out_off, nullptr, oro,
+                                                       nullptr, nullptr, d_w, g->wout, nullptr);
+  PR_TRY(cudaGetLastError());
   PR_TRY(cudaStreamSynchronize(s));
   cleanup();
   return cudaSuccess;

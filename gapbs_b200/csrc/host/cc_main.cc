@@ -32,21 +32,20 @@ std::vector<NodeID> Afforest(const HostGraph &g) {
   return comp;
 }
 
-// src/cc.cc:153-170
-void PrintCompStats(const HostGraph &g, const std::vector<NodeID> &comp) {
-  (void)g;
-  std::cout << std::endl;
-  std::unordered_map<NodeID, NodeID> count;
-  for (NodeID comp_i : comp) count[comp_i] += 1;
-  int k = 5;
-  std::vector<std::pair<NodeID, NodeID>> count_vector;
-  count_vector.reserve(count.size());
-  for (auto kvp : count) count_vector.push_back(kvp);
-  std::vector<std::pair<NodeID, NodeID>> top_k = TopK(count_vector, k);
-  k = std::min(k, static_cast<int>(top_k.size()));
-  std::cout << k << " biggest clusters" << std::endl;
-  for (auto kvp : top_k) std::cout << kvp.second << ":" << kvp.first << std::endl;
-  std::cout << "There are " << count.size() << " components" << std::endl;
+// src/cc.cc:153-170: a blank line, the (at most) five largest components
+// as "label:size" lines, then the number of components.  Sizes are tallied
+// in a hash map and given to TopK in that map's iteration order, as the
+// reference's are: which of several equally large components make the list
+// depends on that order, so the same container and insertion sequence keep
+// the printed lines identical.
+void PrintCompStats(const HostGraph &, const std::vector<NodeID> &comp) {
+  std::unordered_map<NodeID, NodeID> size_of;
+  for (size_t v = 0; v < comp.size(); v++) ++size_of[comp[v]];
+  const std::vector<std::pair<NodeID, NodeID>> sizes(size_of.begin(), size_of.end());
+  const auto largest = TopK(sizes, 5);
+  std::cout << '\n' << largest.size() << " biggest clusters\n";
+  for (const auto &entry : largest) std::cout << entry.second << ':' << entry.first << '\n';
+  std::cout << "There are " << size_of.size() << " components" << std::endl;
 }
 
 // src/cc.cc:173-216: one search per label, as if undirected; every vertex

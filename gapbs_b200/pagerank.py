@@ -15,7 +15,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import byref, c_double, c_int, c_int64
+from ctypes import byref, c_double, c_int, c_int32, c_int64, c_void_p
 from dataclasses import dataclass
 from typing import Optional
 
@@ -100,6 +100,13 @@ class PageRankEngine:
         self.n, self.m = int(n), m
         self.directed = io is not None
         self.weighted = w is not None
+
+    def set_edge_weights_device(self, w_ptr: int):
+        """New edge weights for the weighted graph on the device, from a
+        device pointer to m float32 weights in the uploaded out-CSR order
+        (pr_gpu_set_edge_weights_device): no host copy, no re-upload."""
+        self._check(self._lib.pr_gpu_set_edge_weights_device(self._h, c_void_p(int(w_ptr))),
+                    "pr_gpu_set_edge_weights_device")
 
     def upload(self, g: Graph, edge_w=None):
         if g.num_edges_directed > 0x7FFFFFFF - 8:
@@ -296,6 +303,17 @@ class PageRankEngine:
         return {"blocked": bool(on.value), "slices": sl.value, "bins": bn.value,
                 "pairs": pairs.value, "ids": ids.value, "bytes": nbytes.value,
                 "last_run_blocked": bool(last.value)}
+
+    def sweep_kernel_times(self, max_iters: int = 20, epsilon: float = 1e-4):
+        """One plain solve with every sweep kernel timed on its own
+        (pr_gpu_sweep_kernel_times): the average device ms per sweep of each
+        kernel of the sweep body in launch order, and the sweep count."""
+        ms = (c_double * 3)()
+        nk, sw = c_int(), c_int32()
+        self._check(self._lib.pr_gpu_sweep_kernel_times(self._h, int(max_iters), float(epsilon),
+                                                        ms, 3, byref(nk), byref(sw)),
+                    "pr_gpu_sweep_kernel_times")
+        return [float(ms[k]) for k in range(nk.value)], int(sw.value)
 
     def set_stream(self, stream_handle: Optional[int]):
         """Issue work on a caller stream (raw cudaStream_t), None = own stream."""

@@ -72,6 +72,18 @@ int pr_gpu_upload(pr_gpu_t *h, int64_t n, int64_t m,
                   const int32_t *in_off, const int32_t *in_nbr,
                   const float *edge_w);
 
+/* New edge weights for the weighted graph on the device, from DEVICE memory
+ * on the handle's device: w_dev holds one FP32 weight per entry of the
+ * out-CSR as it was uploaded (the edge_w layout of pr_gpu_upload).  The
+ * weights are checked on the device first (finite and positive, else
+ * PR_GPU_EGRAPH and the previous weights stay); then the per-vertex weight
+ * sums and the engine's two weight arrays are rebuilt by device gathers, in
+ * the handle's stream.  No host copy, no re-upload, no renumbering: a
+ * caller whose weights change every step (a training loop) pays three
+ * device kernels.  A graph uploaded without weights returns PR_GPU_EINVAL.
+ * No counterpart in the reference (its graphs are fixed). */
+int pr_gpu_set_edge_weights_device(pr_gpu_t *h, const float *w_dev);
+
 /* Uploads a serialized graph file (.sg, the layout of src/writer.h:39-69 that
  * the reference's reader loads in src/reader.h:254-307) straight from the
  * file to the device: the file is read in chunks into pinned buffers and
@@ -196,19 +208,24 @@ int pr_gpu_get_batch_tile(const pr_gpu_t *h, int *width);
 /* Sweep layout of single-column solves (plain and personalized PageRank) on
  * unweighted graphs:
  *   PR_GPU_SWEEP_AUTO     slice-blocked when the graph fits that layout's
- *                         limits and the device has room for it, else gather
+ *                         limits, the device has room for it and its
+ *                         in-edges form at most M/2 (row, slice) pairs
+ *                         (skewed graphs such as Kronecker ones; on uniform
+ *                         random graphs nearly every edge is a pair of its
+ *                         own and gather is faster), else gather
  *   PR_GPU_SWEEP_GATHER   one sweep kernel that gathers contrib[v] for every
  *                         in-edge (no extra device memory)
  *   PR_GPU_SWEEP_BLOCKED  slice-blocked; a run on a graph it does not fit
  *                         returns PR_GPU_EINVAL
- * The slice-blocked sweep is two kernels per sweep: per slice of
+ * The slice-blocked sweep is three kernels per sweep: per slice of
  * slice_verts consecutive source vertices (held in shared memory) a partial
- * sum for every destination row the slice reaches, then per bin of rows
- * (bin_words shared-memory words of partials and row sums) the row update.
- * It holds about 2.3 bytes per edge and 14 bytes per (row, slice) pair of
- * extra device memory, built from the device CSR at upload.  slice_verts
- * (multiple of 64, 64..56320) and bin_words (1024..28160): 0 keeps the
- * defaults (49152, 12288).  Changing them rebuilds the layout at the next
+ * sum for every destination row the slice reaches (one launch for the
+ * (row, slice) pairs of 1, 2, 4 or 8 edges, one for the others), then per
+ * bin of rows (bin_words shared-memory words of partials and row sums) the
+ * row update.  It holds about 2.6 bytes per edge and 14 bytes per (row,
+ * slice) pair of extra device memory, built from the device CSR at upload.
+ * slice_verts (multiple of 64, 64..56320) and bin_words (1024..28160): 0
+ * keeps the defaults (49152, 6144).  Changing them rebuilds the layout at the next
  * run.  Weighted graphs, the adjoint and batched solves use gather sweeps.
  * No counterpart in the reference. */
 #define PR_GPU_SWEEP_AUTO 0
@@ -224,6 +241,19 @@ int pr_gpu_set_sweep_layout(pr_gpu_t *h, int layout, int slice_verts, int bin_wo
 int pr_gpu_sweep_layout_info(pr_gpu_t *h, int *blocked, int *slices, int *bins,
                              int64_t *pairs, int64_t *ids, int64_t *bytes,
                              int *last_blocked);
+
+/* Measurement aid: runs one plain PageRank solve of the uploaded graph
+ * (uniform teleport, damping 0.85; scores left in an internal buffer) with
+ * every sweep kernel launched on its own between CUDA events on the
+ * handle's stream, and writes the average device time per sweep of each
+ * kernel of the sweep body, in launch order, to ms[0 .. *nkernels):
+ * slice-blocked: flat-pair partials, other partials, row update; gather:
+ * the sweep kernel.  max_kernels: room in ms (at least 3).  *sweeps_out:
+ * the sweeps the solve ran.  The timings include no loop or launch
+ * overhead of the regular CUDA-graph loop.  No counterpart in the
+ * reference. */
+int pr_gpu_sweep_kernel_times(pr_gpu_t *h, int max_iters, double epsilon, double *ms,
+                              int max_kernels, int *nkernels, int32_t *sweeps_out);
 
 /* Makes the handle issue its work on `stream` (a cudaStream_t of the
  * handle's device, e.g. the caller's framework stream) instead of its own;

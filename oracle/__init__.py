@@ -318,6 +318,10 @@ def ref() -> ctypes.CDLL:
         R.ref_pagerank_pull.restype = None
         R.ref_time_pagerank_pull.argtypes = [P, c_int, c_double, c_int, P]
         R.ref_time_pagerank_pull.restype = c_double
+        R.ref_pagerank_gs.argtypes = [P, c_int, c_double, c_int, P]
+        R.ref_pagerank_gs.restype = None
+        R.ref_time_pagerank_gs.argtypes = [P, c_int, c_double, c_int, P]
+        R.ref_time_pagerank_gs.restype = c_double
         R.ref_pr_verifier.argtypes = [P, P, c_double]
         R.ref_pr_verifier.restype = c_int
         _ref = R
@@ -376,6 +380,17 @@ class RefGraph:
     def time_pagerank_pull(self, trials=1, max_iters=20, epsilon=1e-4):
         per = np.zeros(trials, np.float64)
         tot = ref().ref_time_pagerank_pull(self.h, max_iters, epsilon, trials, _ptr(per))
+        return tot, per
+
+    def pagerank_gs(self, max_iters=20, epsilon=1e-4, logging=False):
+        """The reference's Gauss-Seidel PageRankPullGS (src/pr.cc:34-61)."""
+        s = np.empty(self.num_nodes, np.float32)
+        ref().ref_pagerank_gs(self.h, max_iters, epsilon, int(logging), _ptr(s))
+        return s
+
+    def time_pagerank_gs(self, trials=1, max_iters=20, epsilon=1e-4):
+        per = np.zeros(trials, np.float64)
+        tot = ref().ref_time_pagerank_gs(self.h, max_iters, epsilon, trials, _ptr(per))
         return tot, per
 
     def verify(self, scores, tolerance=1e-4) -> bool:

@@ -7,7 +7,8 @@
 // the result goes to oracle/_ref/ only and is never linked into the product.
 //
 // Entry points wrap: src/pr_spmv.cc PageRankPull (:35-61), PRVerifier
-// (:78-94); src/builder.h BuilderBase::MakeGraph (:343-364);
+// (:78-94); src/pr.cc PageRankPullGS (:34-61); src/builder.h
+// BuilderBase::MakeGraph (:343-364);
 // src/graph.h CSRGraph constructors (:131-151) and GenIndex (:242-249).
 
 #include <chrono>
@@ -15,6 +16,23 @@
 
 #define main gapbs_reference_pr_spmv_main
 #include "pr_spmv.cc"
+#undef main
+
+// The reference's Gauss-Seidel PageRank (src/pr.cc:34-61).  pr.cc defines
+// the same names as pr_spmv.cc (ScoreT, kDamp, PrintTopScores, PRVerifier,
+// main), so it is compiled inside a namespace of its own (the headers it
+// includes are already in, behind their include guards, so only its own
+// definitions land there), with its two functions over Graph renamed so
+// that argument-dependent lookup from its main cannot also find the global
+// ones.
+#define main gapbs_reference_pr_main
+#define PRVerifier PRVerifierGS
+#define PrintTopScores PrintTopScoresGS
+namespace gs {
+#include "pr.cc"
+}  // namespace gs
+#undef PrintTopScores
+#undef PRVerifier
 #undef main
 
 namespace {
@@ -115,6 +133,32 @@ double ref_time_pagerank_pull(void *h, int max_iters, double epsilon,
   for (int t = 0; t < trials; t++) {
     auto t0 = std::chrono::steady_clock::now();
     pvector<ScoreT> s = PageRankPull(g, max_iters, epsilon, false);
+    auto t1 = std::chrono::steady_clock::now();
+    double sec = std::chrono::duration<double>(t1 - t0).count();
+    if (per_trial) per_trial[t] = sec;
+    total += sec;
+  }
+  return total;
+}
+
+// Runs the reference Gauss-Seidel PageRankPullGS; logging prints the
+// per-iteration lines.
+void ref_pagerank_gs(void *h, int max_iters, double epsilon, int logging, float *scores_out) {
+  const Graph &g = static_cast<RefGraph *>(h)->g;
+  pvector<gs::ScoreT> s = gs::PageRankPullGS(g, max_iters, epsilon, logging != 0);
+  std::memcpy(scores_out, s.data(), sizeof(float) * g.num_nodes());
+  std::fflush(stdout);
+}
+
+// Wall-clock seconds of `trials` back-to-back PageRankPullGS calls, as
+// ref_time_pagerank_pull does for the Jacobi kernel.
+double ref_time_pagerank_gs(void *h, int max_iters, double epsilon, int trials,
+                            double *per_trial) {
+  const Graph &g = static_cast<RefGraph *>(h)->g;
+  double total = 0;
+  for (int t = 0; t < trials; t++) {
+    auto t0 = std::chrono::steady_clock::now();
+    pvector<gs::ScoreT> s = gs::PageRankPullGS(g, max_iters, epsilon, false);
     auto t1 = std::chrono::steady_clock::now();
     double sec = std::chrono::duration<double>(t1 - t0).count();
     if (per_trial) per_trial[t] = sec;

@@ -41,7 +41,8 @@ from its own sources by oracle/Makefile) exist.  Writes:
                                      its parent pointers (the depths themselves
                                      for the smallest graphs)
 
-Usage:  python tests/golden/make_golden.py [--fullsize | --cli | --cc | --bfs]
+Usage:  GAPBS_REFERENCE_TREE=<reference source tree> \
+            python tests/golden/make_golden.py [--fullsize | --cli | --cc | --bfs]
 """
 from __future__ import annotations
 
@@ -56,7 +57,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF_TREE = "/root/reference"
+# the reference's source tree (its test/graphs and test/reference fixtures)
+REF_TREE = os.environ.get("GAPBS_REFERENCE_TREE", "")
 sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
@@ -137,8 +139,9 @@ def adversarial_edge_lists():
 
 
 def main():
-    if not os.path.isdir(REF_TREE) or not oracle.ref_available():
-        sys.exit("needs the reference tree and oracle/_ref (make -C oracle)")
+    if not REF_TREE or not os.path.isdir(REF_TREE) or not oracle.ref_available():
+        sys.exit("needs GAPBS_REFERENCE_TREE (the reference source tree) and oracle/_ref "
+                 "(make -C oracle REF=<tree>)")
     gdir = os.path.join(HERE, "graphs")
     os.makedirs(gdir, exist_ok=True)
     for f in GRAPH_FILES:

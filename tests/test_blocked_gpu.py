@@ -161,3 +161,49 @@ def test_layout_argument_checks(engine):
     engine.set_sweep_layout("auto")
     engine.run(20, 1e-4)                              # auto falls back to gather
     assert not engine.sweep_layout_info()["last_run_blocked"]
+
+
+def test_sweep_kernel_times(engine):
+    """pr_gpu_sweep_kernel_times: three kernels per slice-blocked sweep, one
+    per gather sweep, each with a positive time, the same sweep count as a
+    regular solve, and the regular solve's bits unchanged after it."""
+    g = make_graph("-g 14")
+    engine.set_sweep_layout("blocked", 128, 4096)
+    engine.upload(g)
+    before = engine.run(20, 1e-4)
+    ms, sweeps = engine.sweep_kernel_times(20, 1e-4)
+    assert len(ms) == 3 and all(t > 0 for t in ms)
+    assert sweeps == int(before.sweeps[0])
+    after = engine.run(20, 1e-4)
+    assert np.array_equal(before.scores.view(np.uint32), after.scores.view(np.uint32))
+    engine.set_sweep_layout("gather")
+    ms, sweeps = engine.sweep_kernel_times(20, 1e-4)
+    assert len(ms) == 1 and ms[0] > 0 and sweeps == int(before.sweeps[0])
+    with pytest.raises(PageRankError) as ei:
+        engine.sweep_kernel_times(-1, 1e-4)
+    assert ei.value.code == -1
+    engine.set_sweep_layout("auto")
+
+
+def test_auto_keeps_gather_when_pairs_exceed_half_the_edges(engine):
+    """Uniform graph cut into 64-vertex slices: nearly every in-edge is a
+    (row, slice) pair of its own, so PR_GPU_SWEEP_AUTO keeps the gather sweep;
+    PR_GPU_SWEEP_BLOCKED still builds the layout and matches the oracle."""
+    g = make_graph("-u 14")
+    engine.set_sweep_layout("auto", 64, 2048)
+    engine.upload(g)
+    assert not engine.sweep_layout_info()["blocked"]
+    check_plain(engine, g)
+    assert not engine.sweep_layout_info()["last_run_blocked"]
+    engine.set_sweep_layout("blocked", 64, 2048)
+    info = engine.sweep_layout_info()
+    assert info["blocked"] and info["pairs"] > g.num_edges_directed // 2
+    assert info["pairs"] == cpu_pair_count(g, 64)
+    check_plain(engine, g)
+    assert engine.sweep_layout_info()["last_run_blocked"]
+    g2 = make_graph("-g 14")                        # skewed: AUTO takes the layout
+    engine.set_sweep_layout("auto", 64, 2048)
+    engine.upload(g2)
+    info = engine.sweep_layout_info()
+    assert info["blocked"] and info["pairs"] <= g2.num_edges_directed // 2
+    engine.set_sweep_layout("auto")

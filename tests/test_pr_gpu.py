@@ -43,7 +43,10 @@ pytestmark = pytest.mark.gpu
 CASES = ["g10", "u10", "g12", "u12", "g10k4", "g16", "u16", "g18", "el4", "el4s", "mtx4"]
 
 
-LAYOUTS = {"gather": ("gather", 0, 0), "blocked": ("auto", 0, 0),
+# "blocked": the slice-blocked sweep forced (every graph here fits it);
+# "blocked-small": the smallest slices and bins, under the auto rule (which
+# keeps the gather sweep where nearly every edge is a (row, slice) pair)
+LAYOUTS = {"gather": ("gather", 0, 0), "blocked": ("blocked", 0, 0),
            "blocked-small": ("auto", 64, 2048)}
 
 
@@ -79,10 +82,13 @@ def check_parity(engine, g, max_iters=20, epsilon=1e-4, expect_sweeps=None):
     dev = np.abs(res.err_trace[:k32, 0] - tr32)
     assert np.all(dev <= bound), (dev / np.maximum(tr32, 1e-300), bound / np.maximum(tr32, 1e-300))
     layout = getattr(engine, "layout_name", "gather")
+    info = engine.sweep_layout_info()
     if layout == "blocked" and g.num_edges_directed > 0:
-        assert engine.sweep_layout_info()["last_run_blocked"]
+        assert info["last_run_blocked"]
+    if layout == "blocked-small":
+        assert info["last_run_blocked"] == info["blocked"]
     if layout == "gather":
-        assert not engine.sweep_layout_info()["last_run_blocked"]
+        assert not info["last_run_blocked"]
     return res
 
 

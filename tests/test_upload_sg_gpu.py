@@ -2,13 +2,17 @@
 
 A graph written with Graph.write_sg (the reference's .sg layout) and uploaded
 straight from the file must solve exactly as the same graph uploaded from
-host arrays; truncated files and missing files are rejected cleanly.
+host arrays, and both must match the oracle with the plain parity
+tolerances (the reference's sweep count, per vertex 2e-5 relative + 1e-10 of
+FP64, L1 at most 4x the reference's own FP32 L1 + 1e-7, PRVerifier below
+epsilon); truncated files and missing files are rejected cleanly.
 """
 import os
 
 import numpy as np
 import pytest
 
+import oracle
 from gapbs_b200 import PageRankEngine
 from gapbs_b200.graph import Graph, make_graph
 from gapbs_b200.pagerank import PageRankError
@@ -44,6 +48,15 @@ def test_sg_upload_matches_host_upload(engine, kind, tmp_path):
     from_host = engine.run(20, 1e-4)
     assert np.array_equal(from_file.scores, from_host.scores)
     assert np.array_equal(from_file.sweeps, from_host.sweeps)
+    s32, k32, _ = oracle.pr_pull_f32(g, 20, 1e-4)
+    s64, _, _ = oracle.pr_pull_f64(g, 20, 1e-4)
+    assert int(from_file.sweeps[0]) == k32
+    gpu = from_file.scores
+    assert np.all(np.abs(gpu - s64) <= 2e-5 * np.abs(s64) + 1e-10)
+    ref_l1 = float(np.abs(s32.astype(np.float64) - s64).sum())
+    assert float(np.abs(gpu.astype(np.float64) - s64).sum()) <= 4 * ref_l1 + 1e-7
+    if k32 < 20:
+        assert oracle.pr_verify_f32(g, gpu) < 1e-4
 
 
 def test_sg_upload_rejects_bad_files(engine, tmp_path):
