@@ -206,8 +206,9 @@ __device__ __forceinline__ void warp_flat_pairs(const BlockedArgs &a, const uint
   }
 }
 
-// Phase 1: one CTA per SM takes units (a range of the groups of one (slice,
-// class) run) in order from a counter until none is left: the runs of one
+// Phase 1: one CTA per SM takes units (consecutive segments of one slice,
+// each segment a range of the groups of one (slice, class) run) in order
+// from a counter until none is left: the runs of one
 // block per pair (FLAT) or the others, the two kinds being two launches so
 // that each is compiled for its own paths.  When the slice changes the CTA
 // loads the slice's contribs into shared memory (plus a zero at index
@@ -230,10 +231,9 @@ slice_partial_kernel(const BlockedArgs a) {
     __syncthreads();  // also: every warp is done with the previous unit
     const int k = s_unit;
     if (k >= ucount) break;
-    const int4 un = a.unit[ubase + k];  // run, first group, end group
-    const int4 rd = a.run[un.x];        // first group, slice, first id, shape
-    if (rd.y != cur_slice) {
-      const int v0 = rd.y * a.slice_verts;
+    const int4 un = a.unit[ubase + k];  // first segment, end segment, slice
+    if (un.z != cur_slice) {
+      const int v0 = un.z * a.slice_verts;
       const int cnt = min(a.slice_verts, a.nsrc - v0);
       const int n4 = cnt >> 2;
       const float4 *c4 = reinterpret_cast<const float4 *>(a.contrib + v0);
@@ -243,26 +243,33 @@ slice_partial_kernel(const BlockedArgs a) {
         cp_async_4(sv + i, a.contrib + v0 + i);
       if (threadIdx.x == 0) sv[a.slice_verts] = 0.f;
       cp_async_wait_all();
-      cur_slice = rd.y;
+      cur_slice = un.z;
     }
     __syncthreads();  // the slice is in place; s_unit may be overwritten next
-    const int rows = rd.w >> 8, ll = (rd.w >> 4) & 15, lb = rd.w & 15;
-    const int ng = un.z - un.y;
-    // warps split the unit evenly, flat units in whole blocks of 8 / B groups
-    const int q = FLAT ? 8 >> lb : 1;
-    const int per = (ng / q + kSliceWarps - 1) / kSliceWarps * q;
-    const int gw0 = un.y + w * per, gw1 = min(un.z, gw0 + per);
-    if (gw0 >= gw1) continue;
-    const uint16_t *base =
-        a.src + rd.z + (static_cast<int64_t>(gw0 - rd.x) * rows * 32 << lb);
     const unsigned svb = smem_addr(sv);
-    if (FLAT) {
-      warp_flat_pairs(a, base, gw0, gw1 - gw0, lb, svb, ps);
-    } else {
-      switch (lb) {
-        case 1: warp_run_groups<2>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
-        case 2: warp_run_groups<4>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
-        default: warp_run_groups<8>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
+    for (int sg = un.x; sg < un.y; sg++) {
+      const int4 seg = a.seg[sg];          // run, first group, end group
+      const int4 rd = a.run[seg.x];        // first group, slice, first id, shape
+      const int rows = rd.w >> 8, ll = (rd.w >> 4) & 15, lb = rd.w & 15;
+      const int ng = seg.z - seg.y;
+      // warps split each segment evenly (flat segments in whole blocks of
+      // 8 / B groups), the first share going to a different warp for each
+      // segment of the unit so that short segments spread over the warps
+      const int q = FLAT ? 8 >> lb : 1;
+      const int per = (ng / q + kSliceWarps - 1) / kSliceWarps * q;
+      const int wr = (w + 7 * (sg - un.x)) & (kSliceWarps - 1);
+      const int gw0 = seg.y + wr * per, gw1 = min(seg.z, gw0 + per);
+      if (gw0 >= gw1) continue;
+      const uint16_t *base =
+          a.src + rd.z + (static_cast<int64_t>(gw0 - rd.x) * rows * 32 << lb);
+      if (FLAT) {
+        warp_flat_pairs(a, base, gw0, gw1 - gw0, lb, svb, ps);
+      } else {
+        switch (lb) {
+          case 1: warp_run_groups<2>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
+          case 2: warp_run_groups<4>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
+          default: warp_run_groups<8>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
+        }
       }
     }
   }

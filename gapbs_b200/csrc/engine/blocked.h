@@ -71,8 +71,12 @@ struct SliceBlocks {
   // phase 1
   uint16_t *src = nullptr;   // slice-local source ids, sliced-ELL per group
   int4 *run = nullptr;       // {first group, slice, first id, (rows << 8) | (log2 L << 4) | log2 B}
-  // {run, first group, end group, 0}: units of the flat launch, then of
-  // the other; CTAs take them in order from a counter
+  // {run, first group, end group, 0}: pieces of runs, in run order
+  int4 *seg = nullptr;
+  int32_t nsegs = 0;
+  // {first segment, end segment, slice, 0}: units of the flat launch, then
+  // of the other, each consecutive segments of one slice; CTAs take them in
+  // order from a counter
   int4 *unit = nullptr;
   int32_t nunits_flat = 0;
   int32_t *dest = nullptr;   // per pair slot (ngroups x 32): index into part
@@ -99,6 +103,7 @@ struct BlockedArgs {
   // phase 1
   const uint16_t *__restrict__ src;
   const int4 *__restrict__ run;
+  const int4 *__restrict__ seg;
   const int4 *__restrict__ unit;
   int32_t nunits_flat;       // units [0, nunits_flat) flat, [nunits_flat, nunits) the others
   int32_t nunits;

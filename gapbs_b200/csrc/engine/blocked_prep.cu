@@ -28,9 +28,11 @@
 //  5. A stable sort of the pairs by row gives the phase-2 order (row,
 //     slice): per pair its position in its bin's block; row u's pairs are
 //     idx[rowq[u] .. rowq[u + 1]).
-//  6. Phase-1 work is cut, per launch (flat runs / the others), into units:
-//     pieces of one run of about 1 / (6 x CTAs) of the launch's estimated
-//     instruction count; CTAs take units in order from a counter.
+//  6. Phase-1 work is cut, per launch (flat runs / the others), into
+//     segments: pieces of one run of about 1 / (6 x CTAs) of the launch's
+//     estimated instruction count; consecutive segments of one slice are
+//     joined into units up to that size, so that short runs share one load
+//     of their slice; CTAs take units in order from a counter.
 #include <cuda_runtime.h>
 
 #include <cub/cub.cuh>
@@ -306,7 +308,11 @@ __global__ void slot_kernel(int64_t npairs, const int32_t *__restrict__ order,
   const int32_t k = order[i];
   slot_of[k] = slot;
   dest[slot] = ppos[k];
-  atomicMax(run_max + r, pair_len[k]);
+  // run_max: the pairs of a run are consecutive in i, so the lanes of a warp
+  // that share a run join their lengths first and one of them updates it
+  const unsigned peers = __match_any_sync(__activemask(), r);
+  const int32_t len = __reduce_max_sync(peers, static_cast<unsigned>(pair_len[k]));
+  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicMax(run_max + r, len);
   if (rank % per == 0) group_run[grp] = r;
 }
 
@@ -494,7 +500,7 @@ struct CubTemp {
 }  // namespace
 
 void FreeSliceBlocks(SliceBlocks *sb) {
-  void *ptrs[] = {sb->src, sb->run, sb->unit, sb->dest, sb->part,
+  void *ptrs[] = {sb->src, sb->run, sb->seg, sb->unit, sb->dest, sb->part,
                   sb->binbase, sb->idx, sb->rowq, sb->bin};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -774,8 +780,10 @@ cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_word
   bin_table_kernel<<<Blocks(nbins, T), T, 0, s>>>(nbins, bin_row0, pq, sb->bin);
   SB_TRY(cudaGetLastError());
 
-  // 6. phase-1 units: each run cut into pieces of about 1 / (6 G) of its
-  //    launch's estimated work (CTAs take them from a counter)
+  // 6. phase-1 work: each run cut into segments of about 1 / (6 G) of its
+  //    launch's estimated work; consecutive segments of one slice joined
+  //    into units up to that size (so short runs share one slice load);
+  //    CTAs take units from a counter
   const int G = sms;
   std::vector<int32_t> rgb(nruns + 1);
   std::vector<int4> rtab(nruns);
@@ -783,7 +791,7 @@ cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_word
                          cudaMemcpyDeviceToHost, s));
   SB_TRY(cudaMemcpyAsync(rtab.data(), sb->run, sizeof(int4) * nruns, cudaMemcpyDeviceToHost, s));
   SB_TRY(cudaStreamSynchronize(s));
-  std::vector<int4> units;
+  std::vector<int4> segs, units;
   int32_t nunits_flat = 0;
   for (int flat = 1; flat >= 0; flat--) {
     double total = 0;
@@ -791,26 +799,46 @@ cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_word
       if (FlatShape(rtab[r].w) == (flat != 0))
         total += static_cast<double>(GroupCost(rtab[r].w, flat)) * (rgb[r + 1] - rgb[r]);
     const double target = std::max(1.0, total / (6.0 * G));
+    double unit_cost = 0;
     for (int64_t r = 0; r < nruns; r++) {
       if (FlatShape(rtab[r].w) != (flat != 0)) continue;
       const int32_t g0 = rgb[r], g1 = rgb[r + 1];
-      // flat units hold whole blocks of 8 / B groups
+      const double gc = static_cast<double>(GroupCost(rtab[r].w, flat));
+      // flat segments hold whole blocks of 8 / B groups
       const int64_t q = flat ? 8 >> (rtab[r].w & 15) : 1;
-      int64_t per = std::max<int64_t>(
-          1, static_cast<int64_t>(target / static_cast<double>(GroupCost(rtab[r].w, flat))));
+      int64_t per = std::max<int64_t>(1, static_cast<int64_t>(target / gc));
       per = (per + q - 1) / q * q;
-      for (int64_t g = g0; g < g1; g += per)
-        units.push_back(make_int4(static_cast<int32_t>(r), static_cast<int32_t>(g),
-                                  static_cast<int32_t>(std::min<int64_t>(g1, g + per)), 0));
+      for (int64_t g = g0; g < g1; g += per) {
+        const int32_t ge = static_cast<int32_t>(std::min<int64_t>(g1, g + per));
+        const double c = gc * (ge - g);
+        const bool join = !units.empty() && units.back().z == rtab[r].y &&
+                          units.back().y == static_cast<int32_t>(segs.size()) &&
+                          static_cast<int32_t>(units.size()) > (flat ? 0 : nunits_flat) &&
+                          unit_cost + c <= target;
+        segs.push_back(make_int4(static_cast<int32_t>(r), static_cast<int32_t>(g), ge, 0));
+        if (join) {
+          units.back().y++;
+          unit_cost += c;
+        } else {
+          const int32_t sg = static_cast<int32_t>(segs.size()) - 1;
+          units.push_back(make_int4(sg, sg + 1, rtab[r].y, 0));
+          unit_cost = c;
+        }
+      }
     }
     if (flat) nunits_flat = static_cast<int32_t>(units.size());
   }
   const int32_t nunits = static_cast<int32_t>(units.size());
+  const int32_t nsegs = static_cast<int32_t>(segs.size());
+  SB_TRY(Keep(sb, &sb->seg, nsegs));
   SB_TRY(Keep(sb, &sb->unit, nunits));
+  if (nsegs)
+    SB_TRY(cudaMemcpyAsync(sb->seg, segs.data(), sizeof(int4) * nsegs, cudaMemcpyHostToDevice, s));
   if (nunits)
     SB_TRY(cudaMemcpyAsync(sb->unit, units.data(), sizeof(int4) * nunits, cudaMemcpyHostToDevice,
                            s));
-  SB_TRY(cudaStreamSynchronize(s));  // the host vector above feeds an async copy
+  SB_TRY(cudaStreamSynchronize(s));  // the host vectors above feed async copies
+  sb->nsegs = nsegs;
 
   sb->slice_verts = slice_verts;
   sb->bin_words = bin_words;

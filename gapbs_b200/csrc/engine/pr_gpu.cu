@@ -429,6 +429,7 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
     std::memset(&ba, 0, sizeof(ba));
     ba.src = sb.src;
     ba.run = sb.run;
+    ba.seg = sb.seg;
     ba.unit = sb.unit;
     ba.nunits_flat = sb.nunits_flat;
     ba.nunits = sb.nunits;
