@@ -12,9 +12,10 @@
 //     of u is floor(S(u) / W') with S the exclusive scan of the costs and
 //     W' = bin_words - (largest row cost) - 3, so no bin overflows (its block
 //     of partials is rounded up to whole float4) and none is empty.
-//  3. Bin-major position of every pair: a stable sort by (bin, slice, length
-//     class) gives each bin's block of partials, slice-major inside; blocks
-//     start on multiples of four floats.
+//  3. Bin-major position of every pair: a stable sort by (bin, flat class or
+//     not, slice, length class) gives each bin's block of partials: the
+//     pairs of the flat classes (one block of ids per pair) slice-major,
+//     then the others slice-major; blocks start on multiples of four floats.
 //  4. Phase-1 order: a stable sort by (slice, length class).  Each (slice,
 //     class) run is cut into groups of P = 32 / L pairs, L lanes per pair
 //     (1 for short classes, up to 32 for the longest).  A group is a matrix
@@ -211,6 +212,12 @@ __global__ void bin_size_kernel(int32_t nbins, const int32_t *__restrict__ bin_r
   size4[b] = (cnt + 3) & ~3;
 }
 
+// Classes whose runs have one block of B ids per pair and one lane per pair
+// (exact lengths 1, 2, 4 and 8): their runs are flat (FlatShape below).
+__host__ __device__ inline bool ClassFlat(int cls) {
+  return cls == 0 || cls == 1 || cls == 3 || cls == 7;
+}
+
 // Sort keys of the pairs: (bin, slice, class) for the bin-major order and
 // (slice, class) for the phase-1 order; values: pair numbers.
 __global__ void pair_keys_kernel(int64_t npairs, const int32_t *__restrict__ pair_u,
@@ -222,8 +229,12 @@ __global__ void pair_keys_kernel(int64_t npairs, const int32_t *__restrict__ pai
   if (k >= npairs) return;
   const uint64_t cls = static_cast<uint64_t>(PairClass(pair_len[k]));
   const uint64_t c = static_cast<uint64_t>(pair_c[k]);
-  key_bin[k] = (static_cast<uint64_t>(binof[pair_u[k]]) << (sbits + kClassBits)) |
-               (c << kClassBits) | cls;
+  // inside a bin: the pairs of flat classes first, then the others (each
+  // slice-major), so that each phase-1 launch fills one contiguous piece of
+  // every bin, in slice order
+  const uint64_t other = ClassFlat(static_cast<int>(cls)) ? 0 : 1;
+  key_bin[k] = (static_cast<uint64_t>(binof[pair_u[k]]) << (1 + sbits + kClassBits)) |
+               (other << (sbits + kClassBits)) | (c << kClassBits) | cls;
   key_slice[k] = static_cast<uint32_t>((c << kClassBits) | cls);
   val_a[k] = static_cast<int32_t>(k);
   val_b[k] = static_cast<int32_t>(k);
@@ -264,11 +275,6 @@ __global__ void run_start_kernel(int64_t npairs, const int32_t *__restrict__ fla
 // launch of phase 1.
 __host__ __device__ inline bool FlatShape(int code) { return (code >> 4) == 16; }
 
-// Classes whose runs have one block of B ids per pair and one lane per pair
-// (exact lengths 1, 2, 4 and 8): their runs are flat (FlatShape above).
-__host__ __device__ inline bool ClassFlat(int cls) {
-  return cls == 0 || cls == 1 || cls == 3 || cls == 7;
-}
 
 // Groups of each (slice, class) run: its pairs, 32 / lanes to a group; a
 // flat run is padded to whole blocks of 8 / B groups (32 chunks of 16 bytes).
@@ -681,7 +687,7 @@ cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_word
   SB_TRY(cudaGetLastError());
   cub::DoubleBuffer<uint64_t> kbb(kbin[0], kbin[1]);
   cub::DoubleBuffer<int32_t> vab(va[0], va[1]);
-  SB_SORT_PAIRS(kbb, vab, npairs, 0, BitsFor(nbins) + sbits + kClassBits);
+  SB_SORT_PAIRS(kbb, vab, npairs, 0, BitsFor(nbins) + 1 + sbits + kClassBits);
   SB_TRY(tmp.Get(&ppos, npairs));
   bin_pos_kernel<<<Blocks(npairs, T), T, 0, s>>>(npairs, vab.Current(), pair_u, binof, bin_row0,
                                                  pq, sb->binbase, ppos);
