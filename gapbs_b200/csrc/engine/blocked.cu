@@ -30,6 +30,12 @@ __device__ __forceinline__ uint4 ld_stream_u4(const uint4 *p, uint64_t pol) {
 // Shared-memory float at byte address base + 4 i (32-bit shared-window
 // address), so that the compiler issues a shared load with 32-bit address
 // arithmetic whatever it can prove about the pointer it came from.
+__device__ __forceinline__ unsigned lds_u16(unsigned base, unsigned i) {
+  unsigned short v;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(base + (i << 1)));
+  return v;
+}
+
 __device__ __forceinline__ float lds_f32(unsigned base, unsigned i) {
   float v;
   asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(base + (i << 2)));
@@ -277,10 +283,12 @@ slice_partial_kernel(const BlockedArgs a) {
 
 // Phase 2: one CTA per bin of rows (then blocks for the rows without
 // in-edges, on the first sweep only).  The bin's partials, one contiguous
-// block of part[], are copied into shared memory; then each thread takes
-// rows u = row0 + t, + kBinThreads, ...: it sums the row's partials in slice
-// order (their positions in the block: idx[rowq[u] .. rowq[u + 1])) and
-// updates the row.
+// block of part[], and the bin's stretch of idx[] (per pair of its rows, in
+// row order, the pair's position in the block) are copied into shared
+// memory; then each thread takes rows u = row0 + t, + kBinThreads, ...: it
+// sums the row's partials in slice order (positions idx[rowq[u] ..
+// rowq[u + 1])) and updates the row, the next row's own data fetched
+// before this one is written.
 __global__ void __launch_bounds__(kBinThreads)
 bin_row_kernel(const BlockedArgs a) {
   if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
@@ -301,48 +309,60 @@ bin_row_kernel(const BlockedArgs a) {
     const float4 *src4 = reinterpret_cast<const float4 *>(a.part + a.binbase[b]);
     float4 *sm4 = reinterpret_cast<float4 *>(sm);
     for (int i = threadIdx.x; i < np4; i += kBinThreads) cp_async_16(sm4 + i, src4 + i);
-    // the first row's own data is fetched while the block arrives
+    // the bin's positions idx[q0 .. q1) follow the partials in shared
+    // memory, copied in 16-byte words from the one holding idx[q0]
+    const int e0 = q0 & ~7;
+    const int nq = (q1 - e0 + 7) >> 3;
+    uint16_t *sx = reinterpret_cast<uint16_t *>(sm + ((a.bin_words + 3) & ~3));
+    const float4 *idx4 = reinterpret_cast<const float4 *>(a.idx + e0);
+    for (int i = threadIdx.x; i < nq; i += kBinThreads)
+      cp_async_16(reinterpret_cast<float4 *>(sx) + i, idx4 + i);
+    // the first row's own data is fetched while the copies arrive
     int u = row0 + threadIdx.x;
-    int s0 = 0, s1 = 0;
+    int s0 = 0, s1 = 0, deg = 1;
     float old = 0.f;
     if (u < row1) {
-      s0 = a.rowq[u];
-      s1 = a.rowq[u + 1];
+      s0 = a.rowq[u] - e0;
+      s1 = a.rowq[u + 1] - e0;
       old = ld_score(a.score + u, ps);
+      deg = a.odeg ? a.odeg[u] : a.rowoff[u + 1] - a.rowoff[u];
     }
     cp_async_wait_all();
     __syncthreads();
     const unsigned smb = smem_addr(sm);
+    const unsigned sxb = smem_addr(sx);
     while (u < row1) {
       float sum = 0.f;
       int j = s0;
       for (; j + 3 < s1; j += 4) {
-        const unsigned i0 = a.idx[j], i1 = a.idx[j + 1], i2 = a.idx[j + 2], i3 = a.idx[j + 3];
+        const unsigned i0 = lds_u16(sxb, j), i1 = lds_u16(sxb, j + 1);
+        const unsigned i2 = lds_u16(sxb, j + 2), i3 = lds_u16(sxb, j + 3);
         sum = __fadd_rn(sum, lds_f32(smb, i0));
         sum = __fadd_rn(sum, lds_f32(smb, i1));
         sum = __fadd_rn(sum, lds_f32(smb, i2));
         sum = __fadd_rn(sum, lds_f32(smb, i3));
       }
-      for (; j < s1; j++) sum = __fadd_rn(sum, lds_f32(smb, a.idx[j]));
+      for (; j < s1; j++) sum = __fadd_rn(sum, lds_f32(smb, lds_u16(sxb, j)));
       const int un = u + kBinThreads;
-      int n0 = 0, n1 = 0;
+      int n0 = 0, n1 = 0, ndeg = 1;
       float nold = 0.f;
       if (un < row1) {  // the next row's data, fetched before this row is written
-        n0 = a.rowq[un];
-        n1 = a.rowq[un + 1];
+        n0 = a.rowq[un] - e0;
+        n1 = a.rowq[un + 1] - e0;
         nold = ld_score(a.score + un, ps);
+        ndeg = a.odeg ? a.odeg[un] : a.rowoff[un + 1] - a.rowoff[un];
       }
       const float base = a.kind == kKindPPR ? a.base_vec[u] : a.base_scalar;
       // the reference's update: base + d * sum, two roundings (src/pr_spmv.cc:51)
       const float nw = __fadd_rn(base, __fmul_rn(a.damping, sum));
       st_hint_f32(a.score + u, nw, ps);
-      const int deg = a.odeg ? a.odeg[u] : a.rowoff[u + 1] - a.rowoff[u];
       st_hint_f32(a.contrib + u, __fdiv_rn(nw, __int2float_rn(deg)), pl);
       err += static_cast<double>(fabsf(__fsub_rn(nw, old)));
       u = un;
       s0 = n0;
       s1 = n1;
       old = nold;
+      deg = ndeg;
     }
   } else if (it == 0) {
     // rows without in-neighbours: new = base from the first sweep on
@@ -377,6 +397,10 @@ int BinRowGrid(const SliceBlocks &sb, int64_t n) {
 
 // contribs + the zero slot, rounded to whole float4
 size_t SliceSmemBytes(const SliceBlocks &sb) { return sizeof(float) * (sb.slice_verts + 4); }
-size_t BinSmemBytes(const SliceBlocks &sb) { return sizeof(float) * sb.bin_words; }
+// the bin's partials, then its positions (16-byte words from the one
+// holding its first position)
+size_t BinSmemBytes(const SliceBlocks &sb) {
+  return sizeof(float) * ((sb.bin_words + 3) & ~3) + sizeof(uint16_t) * (sb.bin_words + 16);
+}
 
 }  // namespace prgpu

@@ -48,7 +48,7 @@ namespace prgpu {
 constexpr int kSliceWarps = 32;
 constexpr int kBinWarps = 8;
 constexpr int kDefaultSliceVerts = 49152;  // 192 KB of contribs in shared memory
-constexpr int kDefaultBinWords = 6144;     // 24 KB of partials per bin (pairs + rows)
+constexpr int kDefaultBinWords = 6144;     // partials per bin (pairs + rows): 24 KB + 12 KB of positions
 constexpr int kMaxSliceVerts = 56320;      // + the zero slot, within one CTA's shared memory
 constexpr int kMaxPairIds = 2048;          // longer (row, slice) pairs are cut into pieces
 constexpr int kMaxBinWords = 28160;
@@ -111,6 +111,7 @@ struct BlockedArgs {
   int32_t slice_verts;
   int32_t nsrc;
   int32_t part_len;          // floats in part[]
+  int32_t bin_words;         // shared-memory words of partials per bin
   float *part;
   // phase 2
   const int32_t *__restrict__ binbase;

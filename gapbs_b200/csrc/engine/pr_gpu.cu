@@ -438,6 +438,7 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
     ba.nsrc = sb.nsrc;
     ba.part = sb.part;
     ba.part_len = sb.part_len;
+    ba.bin_words = sb.bin_words;
     ba.binbase = sb.binbase;
     ba.idx = sb.idx;
     ba.rowq = sb.rowq;
