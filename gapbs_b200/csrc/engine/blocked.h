@@ -44,11 +44,12 @@
 
 namespace prgpu {
 
-// Phase 1: 1024 threads, one CTA per SM; phase 2: 256 threads per bin.
+// Phase 1: 1024 threads, one CTA per SM; phase 2: 256, 512 or 1024
+// threads per bin (BinRowThreads).
 constexpr int kSliceWarps = 32;
-constexpr int kBinWarps = 8;
 constexpr int kDefaultSliceVerts = 49152;  // 192 KB of contribs in shared memory
 constexpr int kDefaultBinWords = 6144;     // partials per bin (pairs + rows): 24 KB + 12 KB of positions
+constexpr int kLargeBinWords = 12288;      // the default where that leaves >= 64 bins per SM
 constexpr int kMaxSliceVerts = 56320;      // + the zero slot, within one CTA's shared memory
 constexpr int kMaxPairIds = 2048;          // longer (row, slice) pairs are cut into pieces
 constexpr int kMaxBinWords = 28160;
@@ -121,7 +122,7 @@ struct BlockedArgs {
   int32_t nbins;
   int32_t n;                 // vertices (rows [ndst, n) have no in-edges)
   int32_t ndst;
-  int32_t zero_blocks;       // phase-2 blocks after the bins, each for kZeroRowsPerBlock rows
+  int32_t zero_blocks;       // phase-2 blocks after the bins, each for 4 x threads rows
   int32_t kind;              // kKindPlain or kKindPPR
   const int32_t *__restrict__ rowoff;
   const int32_t *__restrict__ odeg;   // directed: out-degree per row; else nullptr
@@ -142,10 +143,9 @@ struct BlockedArgs {
 
 // Phase 1 for the runs of one block per pair (flat) or the others.
 const void *SlicePartialKernel(bool flat);
-const void *BinRowKernel();
+const void *BinRowKernel(const SliceBlocks &sb);
+int BinRowThreads(const SliceBlocks &sb);
 constexpr int kSliceThreads = kSliceWarps * 32;
-constexpr int kBinThreads = kBinWarps * 32;
-constexpr int kZeroRowsPerBlock = kBinThreads * 4;
 // Phase-2 grid: the bins, then blocks for the rows without in-edges.
 int BinRowGrid(const SliceBlocks &sb, int64_t n);
 size_t SliceSmemBytes(const SliceBlocks &sb);

@@ -463,7 +463,7 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
     ba.nblocks = nblocks;
     ba.epsilon = epsilon;
     const void *kf = prgpu::SlicePartialKernel(true), *kr = prgpu::SlicePartialKernel(false);
-    const void *kb = prgpu::BinRowKernel();
+    const void *kb = prgpu::BinRowKernel(sb);
     for (const void *k : {kf, kr})
       PR_CHECK(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(prgpu::SliceSmemBytes(sb))));
@@ -472,7 +472,7 @@ int SolveSingle(pr_gpu_t *h, int max_iters, double epsilon, float damping,
     for (int i = 0; i < 3; i++) {
       body[i].fn = i == 0 ? kf : (i == 1 ? kr : kb);
       body[i].grid = dim3(i < 2 ? sb.nctas : nblocks);
-      body[i].block = dim3(i < 2 ? prgpu::kSliceThreads : prgpu::kBinThreads);
+      body[i].block = dim3(i < 2 ? prgpu::kSliceThreads : prgpu::BinRowThreads(sb));
       body[i].smem = i < 2 ? prgpu::SliceSmemBytes(sb) : prgpu::BinSmemBytes(sb);
       body[i].args = &ba;
       body[i].args_size = sizeof(ba);

@@ -225,7 +225,8 @@ int pr_gpu_get_batch_tile(const pr_gpu_t *h, int *width);
  * row update.  It holds about 2.6 bytes per edge and 14 bytes per (row,
  * slice) pair of extra device memory, built from the device CSR at upload.
  * slice_verts (multiple of 64, 64..56320) and bin_words (1024..28160): 0
- * keeps the defaults (49152, 6144).  Changing them rebuilds the layout at the next
+ * keeps the defaults (49152; 6144, or 12288 on graphs whose pairs and rows
+ * fill at least 64 such bins per SM).  Changing them rebuilds the layout at the next
  * run.  Weighted graphs, the adjoint and batched solves use gather sweeps.
  * No counterpart in the reference. */
 #define PR_GPU_SWEEP_AUTO 0
