@@ -625,6 +625,7 @@ def run_ppr(a, dev):
     for c in range(0, a.ppr_cols, max(1, a.ppr_cols // 8)):
         eng.run_device(a.max_iters, a.epsilon, 0.85, 1, cols[c].data_ptr(), out1.data_ptr())
         maxdiff = max(maxdiff, float((out[:, c] - out1).abs().sum()))
+    schedule = eng.batch_schedule()
     eng.close()
     # Roofline of the batched solve: every column-sweep gathers 4 bytes per
     # edge (one float of each neighbour's contrib row, served mostly by L2);
@@ -658,6 +659,8 @@ def run_ppr(a, dev):
                     "the rate lies between the L2-resident and the 1 GB-array row-gather "
                     "ceilings",
         },
+        "schedule": dict(schedule, chosen_by="autotuner (tile width, then short-row length "
+                                             "and L1 hub budget, timed on the first solve)"),
         "batched_gteps": round(b_gteps, 3),
         "batched_ms": round(b_ms, 3),
         "batched_sweeps_total": int(bsweeps.sum()),

@@ -664,6 +664,13 @@ int MaxTileFor(int64_t n) {
   return kTileWidths[0];
 }
 
+BatchSchedule DefaultSchedule(int Bp) {
+  BatchSchedule d;
+  d.short_len = std::max(kShortLens[0], std::min(kShortLens[4], 1024 / Bp));
+  d.l1_kb = static_cast<int>(kL1GatherBytes / 1024);
+  return d;
+}
+
 int PadWidth(int b) {
   for (int w : kTileWidths)
     if (b <= w) return w;
@@ -769,8 +776,9 @@ int WidthIndex(int Bp) { return Bp == 8 ? 0 : Bp == 16 ? 1 : Bp == 32 ? 2 : 3; }
 // columns' scores are written out at the end of the phase they retired in).
 cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, int max_iters,
                       double epsilon, float damping, int K, int c0, int B, int Bp,
-                      const float *tele_old, float *out_old, int32_t *sweeps_tile,
-                      double *trace_tile, float *sweep_ms, int64_t *launches, std::string *err) {
+                      const BatchSchedule &sched, const float *tele_old, float *out_old,
+                      int32_t *sweeps_tile, double *trace_tile, float *sweep_ms,
+                      int64_t *launches, std::string *err) {
   const int64_t n = g.n;
   const void *fn0 = BatchSweepKernel(g, Bp);
   const int nblocks0 = GridFor(fn0);
@@ -852,13 +860,15 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
     // are processed in the phase's first two sweeps.  Undirected graphs never
     // gather them (no in-neighbour means no out-neighbour).
     a.zero_final_sweep = g.directed ? loops + 2 : 1;
-    a.l1_rows = static_cast<int32_t>(std::min<int64_t>(n, kL1GatherBytes / (4 * tile_bp)));
-    // rows shorter than two rounds of a warp's gathers (2 * kUnroll * 32/L
-    // entries) go one per lane group: bin 1 + log2(L) starts at that length
+    // the schedule of this phase's width (a repack narrows the tile)
+    const BatchSchedule ph = tile_bp == Bp ? sched : ResolveSchedule(bs, tile_bp);
+    a.l1_rows = static_cast<int32_t>(
+        std::min<int64_t>(n, int64_t(1024) * ph.l1_kb / (4 * tile_bp)));
+    // rows shorter than ph.short_len go one per lane group: the degree bin
+    // whose lower bound is short_len starts there
     {
-      const int L = tile_bp / 4;
       int b = 1;
-      for (int l = L; l > 1; l >>= 1) b++;
+      while (b < kBinZero && g.bins.min_len[b - 1] > ph.short_len) b++;
       a.short_start = static_cast<int32_t>(g.bin_row_start[b]);
     }
     a.epsilon = epsilon;
@@ -950,39 +960,83 @@ cudaError_t SolveTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, in
   return cudaSuccess;
 }
 
-// Autotuner: runs two sweeps of the first tile at each supported width and
-// keeps the width with the lowest time per column-sweep.
+// Autotuner: times sweeps of the first tile (one warm sweep that builds the
+// loop graph, then two timed ones) at each supported width with the
+// default schedule and keeps the width with the lowest time per
+// column-sweep; then, at that width, tries half and twice the default
+// short-row length and L1 budgets of 64 and 160 KB, one knob after the
+// other, keeping a change only when it is faster.
 cudaError_t TuneTile(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s, float damping,
                      int ncols, const float *tele_old, std::string *err) {
-  double best = 1e300;
-  int best_w = kMaxTile;
   std::vector<int32_t> sw(kMaxTile);
-  for (int w : kTileWidths) {
+  auto time_one = [&](int w, const BatchSchedule &sch, double *per_col_sweep) {
     const int B = std::min(w, ncols);
-    if (PadWidth(B) != w) continue;     // would waste a wider tile
-    if (w > MaxTileFor(g.n)) continue;  // beyond the gather's 32-bit offsets
     float ms = 0;
     int64_t nl = 0;
-    // one warm sweep (graph build), then a timed two-sweep solve
-    cudaError_t e = SolveTile(g, bs, s, 1, 0.0, damping, ncols, 0, B, w, tele_old, nullptr,
+    cudaError_t e = SolveTile(g, bs, s, 1, 0.0, damping, ncols, 0, B, w, sch, tele_old, nullptr,
                               sw.data(), nullptr, &ms, &nl, err);
     if (e != cudaSuccess) return e;
-    e = SolveTile(g, bs, s, 2, 0.0, damping, ncols, 0, B, w, tele_old, nullptr, sw.data(),
+    e = SolveTile(g, bs, s, 2, 0.0, damping, ncols, 0, B, w, sch, tele_old, nullptr, sw.data(),
                   nullptr, &ms, &nl, err);
     if (e != cudaSuccess) return e;
-    const double per_col_sweep = ms / (2.0 * B);
-    if (per_col_sweep < best) {
-      best = per_col_sweep;
+    *per_col_sweep = ms / (2.0 * B);
+    return cudaSuccess;
+  };
+  double best = 1e300;
+  int best_w = kMaxTile;
+  for (int w : kTileWidths) {
+    if (PadWidth(std::min(w, ncols)) != w) continue;  // would waste a wider tile
+    if (w > MaxTileFor(g.n)) continue;                // beyond the gather's 32-bit offsets
+    double t = 0;
+    cudaError_t e = time_one(w, DefaultSchedule(w), &t);
+    if (e != cudaSuccess) return e;
+    if (t < best) {
+      best = t;
       best_w = w;
     }
   }
+  BatchSchedule cur = DefaultSchedule(best_w);
+  for (int k = 0; k < 2; k++) {
+    const int len = k == 0 ? cur.short_len / 2 : cur.short_len * 2;
+    if (len < kShortLens[0] || len > kShortLens[4]) continue;
+    BatchSchedule c = cur;
+    c.short_len = len;
+    double t = 0;
+    cudaError_t e = time_one(best_w, c, &t);
+    if (e != cudaSuccess) return e;
+    if (t < best) {
+      best = t;
+      cur = c;
+    }
+  }
+  const BatchSchedule by_len = cur;
+  for (int kb : {64, 160}) {
+    BatchSchedule c = by_len;
+    c.l1_kb = kb;
+    double t = 0;
+    cudaError_t e = time_one(best_w, c, &t);
+    if (e != cudaSuccess) return e;
+    if (t < best) {
+      best = t;
+      cur = c;
+    }
+  }
   bs.tuned_tile = best_w;
+  bs.tuned_sched = cur;
   bs.tuned_ncols = ncols;
   bs.tuned_graph = g.rowoff;
   return cudaSuccess;
 }
 
 }  // namespace
+
+BatchSchedule ResolveSchedule(const BatchScratch &bs, int Bp) {
+  BatchSchedule r = DefaultSchedule(Bp);
+  if (bs.tuned_tile == Bp && bs.tuned_sched.short_len) r = bs.tuned_sched;
+  if (bs.sched.short_len) r.short_len = bs.sched.short_len;
+  if (bs.sched.l1_kb) r.l1_kb = bs.sched.l1_kb;
+  return r;
+}
 
 void FreeBatchScratch(BatchScratch *b) {
   for (auto &l : b->loop) l.Reset();
@@ -1013,6 +1067,7 @@ void FreeBatchScratch(BatchScratch *b) {
   b->cap_flag = b->cap_host = 0;
   b->cap_cells = b->cap_cells2 = b->cap_part = b->cap_groups = b->cap_trace = b->cap_seg = 0;
   b->tuned_tile = b->tuned_ncols = 0;
+  b->tuned_sched = BatchSchedule();
   b->tuned_graph = nullptr;
 }
 
@@ -1043,7 +1098,8 @@ cudaError_t SolveBatched(const DeviceGraph &g, BatchScratch &bs, cudaStream_t s,
     const int Bp = PadWidth(B);
     std::fill(trace_tile.begin(), trace_tile.end(), 0.0);
     float ms = 0;
-    cudaError_t e = SolveTile(g, bs, s, max_iters, epsilon, damping, ncols, c0, B, Bp, tele_old,
+    cudaError_t e = SolveTile(g, bs, s, max_iters, epsilon, damping, ncols, c0, B, Bp,
+                              ResolveSchedule(bs, Bp), tele_old,
                               out_old, sweeps_tile.data(), trace_tile.data(), &ms, &nl, err);
     if (e != cudaSuccess) return e;
     sweep_total += ms;

@@ -16,6 +16,19 @@ namespace prgpu {
 constexpr int kMaxTile = 64;
 constexpr int kTileWidths[4] = {8, 16, 32, 64};
 
+// Work schedule of a batched sweep (chosen by the autotuner with the tile
+// width, or set by the caller): rows with fewer than short_len in-entries go
+// one row per lane group of width/4 lanes (the rest one warp per row), and
+// the contribs of the highest-degree rows, l1_kb KB per SM, are gathered
+// through L1 (all others bypass it).  0 = the default for the width:
+// short_len = 1024 / width (two rounds of a warp's gathers), l1_kb = 96.
+struct BatchSchedule {
+  int short_len = 0;
+  int l1_kb = 0;
+};
+// short_len values a schedule may take: the lengths that start a degree bin.
+constexpr int kShortLens[5] = {8, 16, 32, 64, 128};
+
 struct BatchCtl {
   LoopCtl loop;               // done flag + sweep index (see loop_graph.h)
   unsigned tick2;             // stage-2 ticket of the grid reduction
@@ -50,13 +63,19 @@ struct BatchScratch {
   // Column tile width: 0 = chosen by the autotuner (once per uploaded graph
   // and column count), else one of kTileWidths.
   int tile = 0;
+  BatchSchedule sched;      // caller's schedule (0 fields: the autotuner's)
   int tuned_tile = 0;       // autotuner's choice for tuned_ncols
+  BatchSchedule tuned_sched;
   int tuned_ncols = 0;
   const void *tuned_graph = nullptr;
   LoopGraph loop[4];        // one cached sweep-loop graph per tile width
 };
 
 void FreeBatchScratch(BatchScratch *b);
+
+// The schedule a tile of width Bp runs with: the caller's fields where set,
+// else the autotuner's (when tuned for this width), else the defaults.
+BatchSchedule ResolveSchedule(const BatchScratch &bs, int Bp);
 
 // Solves ncols personalized PageRank columns (teleport N x ncols, original
 // ids, device; nullptr = every column uniform 1/N) into out (N x ncols,

@@ -1081,6 +1081,29 @@ int pr_gpu_get_batch_tile(const pr_gpu_t *h, int *width) {
   return PR_GPU_OK;
 }
 
+int pr_gpu_set_batch_schedule(pr_gpu_t *h, int short_len, int l1_kb) {
+  if (!h) return PR_GPU_EINVAL;
+  bool ok_len = short_len == 0;
+  for (int v : prgpu::kShortLens) ok_len = ok_len || v == short_len;
+  if (!ok_len) return SetErr(h, PR_GPU_EINVAL, "short_len must be 0, 8, 16, 32, 64 or 128");
+  if (l1_kb != 0 && (l1_kb < 16 || l1_kb > 224))
+    return SetErr(h, PR_GPU_EINVAL, "l1_kb must be 0 or in [16, 224]");
+  h->bsc.sched.short_len = short_len;
+  h->bsc.sched.l1_kb = l1_kb;
+  return PR_GPU_OK;
+}
+
+int pr_gpu_get_batch_schedule(const pr_gpu_t *h, int *width, int *short_len, int *l1_kb) {
+  if (!h) return PR_GPU_EINVAL;
+  const int w = h->bsc.tile ? h->bsc.tile : h->bsc.tuned_tile;
+  if (width) *width = w;
+  const prgpu::BatchSchedule r =
+      w ? prgpu::ResolveSchedule(h->bsc, w) : prgpu::BatchSchedule();
+  if (short_len) *short_len = w ? r.short_len : h->bsc.sched.short_len;
+  if (l1_kb) *l1_kb = w ? r.l1_kb : h->bsc.sched.l1_kb;
+  return PR_GPU_OK;
+}
+
 int pr_gpu_set_sweep_layout(pr_gpu_t *h, int layout, int slice_verts, int bin_words) {
   if (!h) return PR_GPU_EINVAL;
   if (layout < PR_GPU_SWEEP_AUTO || layout > PR_GPU_SWEEP_BLOCKED)

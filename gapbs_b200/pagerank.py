@@ -284,6 +284,19 @@ class PageRankEngine:
         self._check(self._lib.pr_gpu_get_batch_tile(self._h, byref(w)), "pr_gpu_get_batch_tile")
         return w.value
 
+    def set_batch_schedule(self, short_len: int = 0, l1_kb: int = 0):
+        """Work schedule of batched solves (pr_gpu_set_batch_schedule); 0
+        leaves a field to the autotuner."""
+        self._check(self._lib.pr_gpu_set_batch_schedule(self._h, int(short_len), int(l1_kb)),
+                    "pr_gpu_set_batch_schedule")
+
+    def batch_schedule(self) -> dict:
+        """Tile width and schedule batched solves run with."""
+        w, sl, kb = c_int(), c_int(), c_int()
+        self._check(self._lib.pr_gpu_get_batch_schedule(self._h, byref(w), byref(sl), byref(kb)),
+                    "pr_gpu_get_batch_schedule")
+        return {"tile_width": w.value, "short_len": sl.value, "l1_kb": kb.value}
+
     def set_sweep_layout(self, layout: str = "auto", slice_verts: int = 0, bin_words: int = 0):
         """Sweep layout of single-column solves on unweighted graphs:
         "auto" (slice-blocked when the graph fits it), "gather" or "blocked";

@@ -205,6 +205,20 @@ int pr_gpu_adjoint_device(pr_gpu_t *h, int max_iters, double epsilon,
 int pr_gpu_set_batch_tile(pr_gpu_t *h, int width);
 int pr_gpu_get_batch_tile(const pr_gpu_t *h, int *width);
 
+/* Work schedule of batched solves, chosen by the same autotuner after the
+ * width (at the chosen width it times half and twice the default short-row
+ * length, then L1 budgets of 64 and 160 KB, keeping what is faster):
+ *   short_len  rows with fewer in-entries go one row per group of width/4
+ *              lanes, longer ones one warp per row: 8, 16, 32, 64 or 128
+ *              (default 1024 / width);
+ *   l1_kb      KB per SM of the highest-degree rows' contribs gathered
+ *              through L1, the rest bypassing it: 16..224 (default 96).
+ * 0 leaves a field to the autotuner.  pr_gpu_get_batch_schedule reports
+ * the schedule the current width runs with (the tuned one after the first
+ * batched solve). */
+int pr_gpu_set_batch_schedule(pr_gpu_t *h, int short_len, int l1_kb);
+int pr_gpu_get_batch_schedule(const pr_gpu_t *h, int *width, int *short_len, int *l1_kb);
+
 /* Sweep layout of single-column solves (plain and personalized PageRank) on
  * unweighted graphs:
  *   PR_GPU_SWEEP_AUTO     slice-blocked when the graph fits that layout's

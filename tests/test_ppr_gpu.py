@@ -109,3 +109,32 @@ def test_directed_ppr(engine):
     T = seed_teleports(g, 4, rng)
     res = engine.run(20, 1e-4, teleport=T)
     check_columns(g, T, res)
+
+
+def test_batched_schedules(engine):
+    """Every work schedule gives the oracle's columns (the schedule only moves
+    rows between the lane-group and warp-per-row paths and hub rows in or
+    out of L1); the autotuner's choice is one of the allowed values; bad
+    settings are refused with PR_GPU_EINVAL."""
+    from gapbs_b200.pagerank import PageRankError
+    g = make_graph("-g 14")
+    engine.upload(g)
+    T = seed_teleports(g, 16, np.random.default_rng(6))
+    for short_len, l1_kb in [(8, 16), (128, 224), (32, 64)]:
+        engine.set_batch_schedule(short_len, l1_kb)
+        engine.set_batch_tile(16)
+        res = engine.run(20, 1e-4, teleport=T)
+        sch = engine.batch_schedule()
+        assert sch == {"tile_width": 16, "short_len": short_len, "l1_kb": l1_kb}
+        check_columns(g, T, res)
+    engine.set_batch_schedule(0, 0)
+    engine.set_batch_tile(0)
+    res = engine.run(20, 1e-4, teleport=T)
+    sch = engine.batch_schedule()
+    assert sch["tile_width"] in (8, 16)
+    assert sch["short_len"] in (8, 16, 32, 64, 128) and 16 <= sch["l1_kb"] <= 224
+    check_columns(g, T, res)
+    for bad in [(12, 0), (0, 8), (0, 300)]:
+        with pytest.raises(PageRankError) as ei:
+            engine.set_batch_schedule(*bad)
+        assert ei.value.code == -1
