@@ -321,6 +321,9 @@ def run_ours(a, dist: Dist):
     sweeps_per_step = sweeps_total / a.steps
     edges_all = dist.sum(float(m) * sweeps_total)
     value = edges_all / (max_ms / 1e3) / 1e9
+    # the sweep layout the timed solves ran with
+    layout = eng.sweep_layout_info()
+    blocked = layout["last_run_blocked"]
 
     # ---- end to end through the C-ABI host call (pinned host result buffer)
     eng.set_stream(None)
@@ -439,12 +442,11 @@ def run_ours(a, dist: Dist):
     bps = sweep_bytes(n, m, directed)
     avg_sweep_ms = sweep_ms_total / max(sweeps_total, 1)
     achieved = bps / (avg_sweep_ms / 1e3) / 1e9
-    layout = eng.sweep_layout_info()
-    blocked = layout["last_run_blocked"]
     traffic = profiled_traffic(a.graph, blocked)
     # each kernel of the sweep body timed on its own (CUDA events between
     # separate launches, one extra solve outside the timed region)
     kms, ksweeps = eng.sweep_kernel_times(a.max_iters, a.epsilon)
+    assert len(kms) == (3 if blocked else 1), "sweep layout changed between legs"
     knames = (["slice_partial_kernel<flat pairs>", "slice_partial_kernel<other pairs>",
                "bin_row_kernel"] if blocked else ["pull_sweep_kernel"])
     kernels = [{"kernel": kn, "ms_per_sweep": round(t, 4), "share": round(t / sum(kms), 4)}
