@@ -3,7 +3,8 @@
 For each graph: sweeps (GPU / reference FP32 restatement), L1 and max-abs
 error of the GPU scores against the FP64 oracle, the same for the
 reference's FP32 scores (the oracle's bit-exact restatement of
-src/pr_spmv.cc:35-61), and the PRVerifier total error of the GPU scores.
+src/pr_spmv.cc:35-61), the PRVerifier total error of the GPU scores, and the
+sweep layout the engine used (slice-blocked or gather, its default choice).
 Prints a markdown table.  Needs a GPU; run as `python tests/parity_report.py`.
 """
 import os
@@ -25,8 +26,8 @@ GRAPHS = ["-g 10", "-u 10", "-g 12", "-u 12", "-g 16", "-u 16", "-g 18", "-u 18"
 def main():
     eng = PageRankEngine(0)
     print("| graph | N | M | sweeps GPU / ref | L1(GPU-fp64) | max abs(GPU-fp64) "
-          "| L1(ref fp32-fp64) | max abs(ref-fp64) | PRVerifier error (GPU) |")
-    print("|---|---:|---:|---|---:|---:|---:|---:|---:|")
+          "| L1(ref fp32-fp64) | max abs(ref-fp64) | PRVerifier error (GPU) | sweep |")
+    print("|---|---:|---:|---|---:|---:|---:|---:|---:|---|")
     for args in GRAPHS:
         g = make_graph(args)
         eng.upload(g)
@@ -38,7 +39,8 @@ def main():
         ver = oracle.pr_verify_f32(g, res.scores)
         print(f"| `{args}` | {g.num_nodes} | {g.num_edges_directed} | {int(res.sweeps[0])} / {k32} "
               f"| {np.abs(s - s64).sum():.3e} | {np.abs(s - s64).max():.3e} "
-              f"| {np.abs(r - s64).sum():.3e} | {np.abs(r - s64).max():.3e} | {ver:.3e} |",
+              f"| {np.abs(r - s64).sum():.3e} | {np.abs(r - s64).max():.3e} | {ver:.3e} "
+              f"| {'slice-blocked' if eng.sweep_layout_info()['last_run_blocked'] else 'gather'} |",
               flush=True)
     eng.close()
 
