@@ -11,7 +11,7 @@
 //     slice_verts consecutive (renumbered) source ids in shared memory.  The
 //     in-edges of one row from one slice form a pair; the slice's pairs are
 //     stored sliced-ELL: grouped by length class into groups of 32 lanes,
-//     L lanes per pair (1 for short pairs, up to 32 for the longest), the
+//     L lanes per pair (1 to 32, chosen per run of a class), the
 //     16-bit slice-local source ids of each lane's share interleaved across
 //     the group in blocks of B ids (B = 1, 2, 4 or 8 by length, padded with
 //     an id whose value is zero).  All groups of one (slice, class) run

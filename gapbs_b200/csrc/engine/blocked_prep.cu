@@ -18,7 +18,8 @@
 //     then the others slice-major; blocks start on multiples of four floats.
 //  4. Phase-1 order: a stable sort by (slice, length class).  Each (slice,
 //     class) run is cut into groups of P = 32 / L pairs, L lanes per pair
-//     (1 for short classes, up to 32 for the longest).  A group is a matrix
+//     (1..32, chosen per run from its pair count and its longest pair by
+//     an instruction estimate, RunLogL).  A group is a matrix
 //     of rows x 32 lanes of blocks of B ids (B = 1, 2, 4 or 8 by class):
 //     block j of the group's pair p sits in row j / L, lane p L + j % L;
 //     rows = the blocks of the run's longest pair over L, rounded up, the
@@ -77,18 +78,6 @@ __host__ __device__ inline int ClassLogB(int cls) {
   if (cls >= 3) return 2;   // 4..7
   if (cls >= 1) return 1;   // 2..3
   return 0;                 // 1
-}
-
-// log2 of the lanes that share one pair of a class (blocks of 8 ids: up to
-// 2 -> 1 lane, 3..4 -> 2, 5..8 -> 4, 9..15 -> 8, 16..31 -> 16, more -> 32);
-// a group holds 32 / lanes pairs.
-__host__ __device__ inline int ClassLogL(int cls) {
-  if (cls <= 8) return 0;
-  if (cls <= 10) return 1;
-  if (cls <= 14) return 2;
-  if (cls <= 18) return 3;
-  if (cls <= 22) return 4;
-  return 5;
 }
 
 __global__ void rowid_kernel(int32_t ndst, const int32_t *__restrict__ rowoff, int32_t *rowid) {
@@ -240,6 +229,34 @@ __global__ void pair_keys_kernel(int64_t npairs, const int32_t *__restrict__ pai
   val_b[k] = static_cast<int32_t>(k);
 }
 
+// log2 of the lanes L that share one pair of a run, chosen per run from its
+// pair count P and its longest pair (nb blocks of B ids): a group holds
+// 32 / L pairs and rows = ceil(nb / L) blocks per lane, so small L pads
+// fewer ids (rows round up less) but leaves pair slots of a short run empty
+// and large L the reverse.  The choice minimises the estimated instructions
+// of the run, per lane: groups x (rows x (4 B + 6) + 2 B + 3 log2 L + 10)
+// (a block's loads and sums per row, the group's closing tree, shuffles and
+// store), ties to the larger L.  Flat classes keep one lane (one block per
+// pair); for the others L = 1 still gives rows >= 2 (their pairs have at
+// least two blocks), so their runs never take the flat shape.
+__host__ __device__ inline int RunLogL(int cls, int64_t npairs, int nb) {
+  if (ClassFlat(cls)) return 0;
+  const int64_t B = int64_t(1) << ClassLogB(cls);
+  int best_ll = 0;
+  int64_t best = -1;
+  for (int ll = 0; ll <= 5; ll++) {
+    const int64_t per = 32 >> ll;
+    const int64_t groups = (npairs + per - 1) / per;
+    const int64_t rows = (nb + (1 << ll) - 1) >> ll;
+    const int64_t c = groups * (rows * (4 * B + 6) + 2 * B + 3 * ll + 10);
+    if (best < 0 || c <= best) {
+      best = c;
+      best_ll = ll;
+    }
+  }
+  return best_ll;
+}
+
 // Bin-major position of the pair at sorted rank r: its bin's base plus its
 // rank inside the bin (the pairs of a bin's rows are consecutive ranks,
 // starting at pq[row0]).
@@ -276,16 +293,45 @@ __global__ void run_start_kernel(int64_t npairs, const int32_t *__restrict__ fla
 __host__ __device__ inline bool FlatShape(int code) { return (code >> 4) == 16; }
 
 
-// Groups of each (slice, class) run: its pairs, 32 / lanes to a group; a
-// flat run is padded to whole blocks of 8 / B groups (32 chunks of 16 bytes).
-__global__ void run_groups_kernel(int32_t nruns, int64_t npairs,
-                                  const int32_t *__restrict__ run_start,
-                                  const uint32_t *__restrict__ key, int32_t *run_groups) {
+// The longest pair of each run: the pairs of a run are consecutive in the
+// phase-1 order, so the lanes of a warp that share a run join their lengths
+// first and one of them updates it.
+__global__ void run_max_kernel(int64_t npairs, const int32_t *__restrict__ order,
+                               const int32_t *__restrict__ run_incl,
+                               const int32_t *__restrict__ pair_len, int32_t *run_max) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= npairs) return;
+  const int32_t r = run_incl[i] - 1;
+  const unsigned peers = __match_any_sync(__activemask(), r);
+  const int32_t len = __reduce_max_sync(peers, static_cast<unsigned>(pair_len[order[i]]));
+  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicMax(run_max + r, len);
+}
+
+// Lanes per pair of each run (RunLogL).
+__global__ void run_lanes_kernel(int32_t nruns, int64_t npairs,
+                                 const int32_t *__restrict__ run_start,
+                                 const uint32_t *__restrict__ key,
+                                 const int32_t *__restrict__ run_max, int32_t *run_ll) {
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= nruns) return;
   const int64_t end = r + 1 < nruns ? run_start[r + 1] : npairs;
   const int cls = static_cast<int>(key[run_start[r]] & ((1u << kClassBits) - 1));
-  const int per = 32 >> ClassLogL(cls);
+  const int lb = ClassLogB(cls);
+  const int nb = (run_max[r] + (1 << lb) - 1) >> lb;
+  run_ll[r] = RunLogL(cls, end - run_start[r], nb);
+}
+
+// Groups of each (slice, class) run: its pairs, 32 / lanes to a group; a
+// flat run is padded to whole blocks of 8 / B groups (32 chunks of 16 bytes).
+__global__ void run_groups_kernel(int32_t nruns, int64_t npairs,
+                                  const int32_t *__restrict__ run_start,
+                                  const uint32_t *__restrict__ key,
+                                  const int32_t *__restrict__ run_ll, int32_t *run_groups) {
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= nruns) return;
+  const int64_t end = r + 1 < nruns ? run_start[r + 1] : npairs;
+  const int cls = static_cast<int>(key[run_start[r]] & ((1u << kClassBits) - 1));
+  const int per = 32 >> run_ll[r];
   int32_t groups = static_cast<int32_t>((end - run_start[r] + per - 1) / per);
   if (ClassFlat(cls)) {
     const int q = 8 >> ClassLogB(cls);
@@ -295,30 +341,24 @@ __global__ void run_groups_kernel(int32_t nruns, int64_t npairs,
 }
 
 // Slot of the pair at phase-1 rank i (group * 32 + its place in the group);
-// the longest pair of its run; the run of each group.
+// the run of each group.
 __global__ void slot_kernel(int64_t npairs, const int32_t *__restrict__ order,
                             const int32_t *__restrict__ run_incl,
                             const int32_t *__restrict__ run_start,
                             const int32_t *__restrict__ run_gbase,
-                            const uint32_t *__restrict__ key, const int32_t *__restrict__ pair_len,
-                            const int32_t *__restrict__ ppos, int32_t *slot_of, int32_t *run_max,
+                            const int32_t *__restrict__ run_ll,
+                            const int32_t *__restrict__ ppos, int32_t *slot_of,
                             int32_t *group_run, int32_t *dest) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= npairs) return;
   const int32_t r = run_incl[i] - 1;
-  const int cls = static_cast<int>(key[i] & ((1u << kClassBits) - 1));
-  const int per = 32 >> ClassLogL(cls);
+  const int per = 32 >> run_ll[r];
   const int32_t rank = static_cast<int32_t>(i - run_start[r]);
   const int32_t grp = run_gbase[r] + rank / per;
   const int32_t slot = grp * 32 + rank % per;
   const int32_t k = order[i];
   slot_of[k] = slot;
   dest[slot] = ppos[k];
-  // run_max: the pairs of a run are consecutive in i, so the lanes of a warp
-  // that share a run join their lengths first and one of them updates it
-  const unsigned peers = __match_any_sync(__activemask(), r);
-  const int32_t len = __reduce_max_sync(peers, static_cast<unsigned>(pair_len[k]));
-  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicMax(run_max + r, len);
   if (rank % per == 0) group_run[grp] = r;
 }
 
@@ -327,6 +367,7 @@ __global__ void slot_kernel(int64_t npairs, const int32_t *__restrict__ order,
 __global__ void run_shape_kernel(int32_t nruns, const int32_t *__restrict__ run_start,
                                  const uint32_t *__restrict__ key,
                                  const int32_t *__restrict__ run_max,
+                                 const int32_t *__restrict__ run_ll,
                                  const int32_t *__restrict__ run_groups, int32_t *run_code,
                                  int64_t *run_gsize, int64_t *run_ids) {
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -336,7 +377,7 @@ __global__ void run_shape_kernel(int32_t nruns, const int32_t *__restrict__ run_
     return;
   }
   const int cls = static_cast<int>(key[run_start[r]] & ((1u << kClassBits) - 1));
-  const int lb = ClassLogB(cls), ll = ClassLogL(cls);
+  const int lb = ClassLogB(cls), ll = run_ll[r];
   const int nb = (run_max[r] + (1 << lb) - 1) >> lb;
   const int rows = (nb + (1 << ll) - 1) >> ll;
   run_code[r] = (rows << 8) | (ll << 4) | lb;
@@ -724,7 +765,15 @@ cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_word
   SB_TRY(tmp.Get(&run_groups, nruns + 1));
   SB_TRY(tmp.Get(&run_gbase, nruns + 1));
   run_start_kernel<<<Blocks(npairs, T), T, 0, s>>>(npairs, rflag, rincl, run_start);
-  run_groups_kernel<<<Blocks(nruns, T), T, 0, s>>>(nruns, npairs, run_start, key1, run_groups);
+  int32_t *run_max = nullptr, *run_ll = nullptr;
+  SB_TRY(tmp.Get(&run_max, nruns));
+  SB_TRY(tmp.Get(&run_ll, nruns));
+  SB_TRY(cudaMemsetAsync(run_max, 0, sizeof(int32_t) * nruns, s));
+  run_max_kernel<<<Blocks(npairs, T), T, 0, s>>>(npairs, order1, rincl, pair_len, run_max);
+  run_lanes_kernel<<<Blocks(nruns, T), T, 0, s>>>(nruns, npairs, run_start, key1, run_max,
+                                                   run_ll);
+  run_groups_kernel<<<Blocks(nruns, T), T, 0, s>>>(nruns, npairs, run_start, key1, run_ll,
+                                                   run_groups);
   SB_TRY(cudaMemsetAsync(run_groups + nruns, 0, sizeof(int32_t), s));
   SB_SCAN(ExclusiveSum, run_groups, run_gbase, nruns + 1);
   int32_t ngroups = 0;
@@ -735,23 +784,20 @@ cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_word
     return cudaSuccess;
   }
   const int32_t nslots = ngroups * 32;
-  int32_t *slot_of = nullptr, *run_max = nullptr, *group_run = nullptr, *run_code = nullptr;
+  int32_t *slot_of = nullptr, *group_run = nullptr, *run_code = nullptr;
   int64_t *run_gsize = nullptr, *run_ids = nullptr, *run_ibase = nullptr;
   SB_TRY(tmp.Get(&slot_of, npairs));
-  SB_TRY(tmp.Get(&run_max, nruns));
   SB_TRY(tmp.Get(&group_run, ngroups));
   SB_TRY(tmp.Get(&run_code, nruns));
   SB_TRY(tmp.Get(&run_gsize, nruns));
   SB_TRY(tmp.Get(&run_ids, nruns + 1));
   SB_TRY(tmp.Get(&run_ibase, nruns + 1));
   SB_TRY(Keep(sb, &sb->dest, nslots));
-  SB_TRY(cudaMemsetAsync(run_max, 0, sizeof(int32_t) * nruns, s));
   fill_i32_kernel<<<Blocks(nslots, T), T, 0, s>>>(nslots, part_len - 4, sb->dest);  // junk slot
-  slot_kernel<<<Blocks(npairs, T), T, 0, s>>>(npairs, order1, rincl, run_start, run_gbase, key1,
-                                              pair_len, ppos, slot_of, run_max, group_run,
-                                              sb->dest);
-  run_shape_kernel<<<Blocks(nruns + 1, T), T, 0, s>>>(nruns, run_start, key1, run_max, run_groups,
-                                                      run_code, run_gsize, run_ids);
+  slot_kernel<<<Blocks(npairs, T), T, 0, s>>>(npairs, order1, rincl, run_start, run_gbase, run_ll,
+                                              ppos, slot_of, group_run, sb->dest);
+  run_shape_kernel<<<Blocks(nruns + 1, T), T, 0, s>>>(nruns, run_start, key1, run_max, run_ll,
+                                                      run_groups, run_code, run_gsize, run_ids);
   SB_TRY(cudaGetLastError());
   SB_SCAN(ExclusiveSum, run_ids, run_ibase, nruns + 1);
   int64_t elems = 0;
