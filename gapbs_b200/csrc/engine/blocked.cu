@@ -212,22 +212,32 @@ __device__ __forceinline__ void warp_flat_pairs(const BlockedArgs &a, const uint
   }
 }
 
+// Groups in one chunk of a phase-1 segment of the given run shape: flat
+// runs two blocks of 32 chunks of 16 bytes (2 x 8 / B groups); the others
+// enough groups for about 16 rows of items per lane.
+template <bool FLAT>
+__device__ __forceinline__ int ChunkGroups(int code) {
+  if (FLAT) return 2 * (8 >> (code & 15));
+  const int rows = code >> 8;
+  return rows >= 16 ? 1 : 16 / rows;
+}
+
 // Phase 1: one CTA per SM takes units (consecutive segments of one slice,
 // each segment a range of the groups of one (slice, class) run) in order
 // from a counter until none is left: the runs of one
 // block per pair (FLAT) or the others, the two kinds being two launches so
 // that each is compiled for its own paths.  When the slice changes the CTA
 // loads the slice's contribs into shared memory (plus a zero at index
-// slice_verts, the id of padding entries); each warp takes an equal share of
-// the unit's groups.
+// slice_verts, the id of padding entries); its warps take chunks of the
+// unit from a shared counter, so that they finish the unit together.
 template <bool FLAT>
 __global__ void __launch_bounds__(kSliceThreads, 1)
 slice_partial_kernel(const BlockedArgs a) {
   if (*reinterpret_cast<volatile const int *>(&a.ctl->loop.done)) return;
   extern __shared__ __align__(16) float sv[];
   __shared__ int s_unit;
+  __shared__ int s_chunk;  // next chunk of the current unit
   const uint64_t ps = policy_evict_first();
-  const int w = threadIdx.x >> 5;
   int cur_slice = -1;
   const int ubase = FLAT ? 0 : a.nunits_flat;
   const int ucount = FLAT ? a.nunits_flat : a.nunits - a.nunits_flat;
@@ -237,6 +247,9 @@ slice_partial_kernel(const BlockedArgs a) {
     __syncthreads();  // also: every warp is done with the previous unit
     const int k = s_unit;
     if (k >= ucount) break;
+    // no warp takes chunks of the previous unit any more: restart the count
+    // (read only after the barrier below)
+    if (threadIdx.x == 0) s_chunk = 0;
     const int4 un = a.unit[ubase + k];  // first segment, end segment, slice
     if (un.z != cur_slice) {
       const int v0 = un.z * a.slice_verts;
@@ -253,19 +266,30 @@ slice_partial_kernel(const BlockedArgs a) {
     }
     __syncthreads();  // the slice is in place; s_unit may be overwritten next
     const unsigned svb = smem_addr(sv);
-    for (int sg = un.x; sg < un.y; sg++) {
-      const int4 seg = a.seg[sg];          // run, first group, end group
-      const int4 rd = a.run[seg.x];        // first group, slice, first id, shape
+    // warps take chunks of the unit from a shared counter until none is
+    // left: a chunk is a few groups of one segment (flat segments: whole
+    // blocks of 8 / B groups), found by walking the unit's segments
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+      int c = 0;
+      if (lane == 0) c = atomicAdd(&s_chunk, 1);
+      c = __shfl_sync(kFull, c, 0);
+      int sg = un.x, gw0 = 0, gw1 = 0;
+      int4 rd = make_int4(0, 0, 0, 0);
+      for (; sg < un.y; sg++) {
+        const int4 seg = a.seg[sg];  // run, first group, end group
+        rd = a.run[seg.x];           // first group, slice, first id, shape
+        const int cg = ChunkGroups<FLAT>(rd.w);
+        const int nch = (seg.z - seg.y + cg - 1) / cg;
+        if (c < nch) {
+          gw0 = seg.y + c * cg;
+          gw1 = min(seg.z, gw0 + cg);
+          break;
+        }
+        c -= nch;
+      }
+      if (sg >= un.y) break;
       const int rows = rd.w >> 8, ll = (rd.w >> 4) & 15, lb = rd.w & 15;
-      const int ng = seg.z - seg.y;
-      // warps split each segment evenly (flat segments in whole blocks of
-      // 8 / B groups), the first share going to a different warp for each
-      // segment of the unit so that short segments spread over the warps
-      const int q = FLAT ? 8 >> lb : 1;
-      const int per = (ng / q + kSliceWarps - 1) / kSliceWarps * q;
-      const int wr = (w + 7 * (sg - un.x)) & (kSliceWarps - 1);
-      const int gw0 = seg.y + wr * per, gw1 = min(seg.z, gw0 + per);
-      if (gw0 >= gw1) continue;
       const uint16_t *base =
           a.src + rd.z + (static_cast<int64_t>(gw0 - rd.x) * rows * 32 << lb);
       if (FLAT) {

@@ -236,18 +236,23 @@ __global__ void pair_keys_kernel(int64_t npairs, const int32_t *__restrict__ pai
 // and large L the reverse.  The choice minimises the estimated instructions
 // of the run, per lane: groups x (rows x (4 B + 6) + 2 B + 3 log2 L + 10)
 // (a block's loads and sums per row, the group's closing tree, shuffles and
-// store), ties to the larger L.  Flat classes keep one lane (one block per
-// pair); for the others L = 1 still gives rows >= 2 (their pairs have at
-// least two blocks), so their runs never take the flat shape.
+// store), ties to the larger L, among the L that keep rows at most
+// kMaxRunRows (or L = 32): one lane per long pair would leave few groups,
+// and so few busy warps, on all but the largest graphs.  Flat classes keep
+// one lane (one block per pair); for the others L = 1 still gives rows >= 2
+// (their pairs have at least two blocks), so their runs never take the flat
+// shape.
+constexpr int kMaxRunRows = 16;
 __host__ __device__ inline int RunLogL(int cls, int64_t npairs, int nb) {
   if (ClassFlat(cls)) return 0;
   const int64_t B = int64_t(1) << ClassLogB(cls);
-  int best_ll = 0;
+  int best_ll = 5;
   int64_t best = -1;
   for (int ll = 0; ll <= 5; ll++) {
     const int64_t per = 32 >> ll;
     const int64_t groups = (npairs + per - 1) / per;
     const int64_t rows = (nb + (1 << ll) - 1) >> ll;
+    if (rows > kMaxRunRows && ll < 5) continue;
     const int64_t c = groups * (rows * (4 * B + 6) + 2 * B + 3 * ll + 10);
     if (best < 0 || c <= best) {
       best = c;
