@@ -221,7 +221,9 @@ int pr_gpu_get_batch_schedule(const pr_gpu_t *h, int *width, int *short_len, int
 
 /* Sweep layout of single-column solves (plain and personalized PageRank) on
  * unweighted graphs:
- *   PR_GPU_SWEEP_AUTO     slice-blocked when the graph fits that layout's
+ *   PR_GPU_SWEEP_AUTO     slice-blocked when the graph has at least 48 Mi
+ *                         (48 x 2^20) edges (below that the gather sweep's
+ *                         contribs stay in the caches), fits that layout's
  *                         limits, the device has room for it and its
  *                         in-edges form at most M/2 (row, slice) pairs
  *                         (skewed graphs such as Kronecker ones; on uniform

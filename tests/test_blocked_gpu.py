@@ -185,10 +185,12 @@ def test_sweep_kernel_times(engine):
     engine.set_sweep_layout("auto")
 
 
-def test_auto_keeps_gather_when_pairs_exceed_half_the_edges(engine):
-    """Uniform graph cut into 64-vertex slices: nearly every in-edge is a
-    (row, slice) pair of its own, so PR_GPU_SWEEP_AUTO keeps the gather sweep;
-    PR_GPU_SWEEP_BLOCKED still builds the layout and matches the oracle."""
+def test_auto_rule(engine):
+    """PR_GPU_SWEEP_AUTO keeps the gather sweep on graphs below 48 Mi edges
+    and where nearly every in-edge is a (row, slice) pair of its own (a
+    uniform graph cut into 64-vertex slices), where PR_GPU_SWEEP_BLOCKED
+    still builds the layout and matches the oracle; it takes the layout on
+    a Kronecker graph of 64 M edges."""
     g = make_graph("-u 14")
     engine.set_sweep_layout("auto", 64, 2048)
     engine.upload(g)
@@ -201,9 +203,11 @@ def test_auto_keeps_gather_when_pairs_exceed_half_the_edges(engine):
     assert info["pairs"] == cpu_pair_count(g, 64)
     check_plain(engine, g)
     assert engine.sweep_layout_info()["last_run_blocked"]
-    g2 = make_graph("-g 14")                        # skewed: AUTO takes the layout
-    engine.set_sweep_layout("auto", 64, 2048)
-    engine.upload(g2)
-    info = engine.sweep_layout_info()
-    assert info["blocked"] and info["pairs"] <= g2.num_edges_directed // 2
     engine.set_sweep_layout("auto")
+    engine.upload(make_graph("-g 14"))              # small: gather
+    assert not engine.sweep_layout_info()["blocked"]
+    n, m = engine.generate("-g 21")                 # 64 M edges, skewed: the layout
+    info = engine.sweep_layout_info()
+    assert m >= 48 << 20 and info["blocked"] and info["pairs"] <= m // 2
+    res = engine.run(20, 1e-4)
+    assert engine.sweep_layout_info()["last_run_blocked"] and int(res.sweeps[0]) > 0
