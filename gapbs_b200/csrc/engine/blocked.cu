@@ -65,28 +65,9 @@ __device__ __forceinline__ void cp_async_wait_all() {
 
 
 
-// The block of B ids (B = 2, 4, 8) a lane reads for one row of a group, in
-// its natural width, and the contrib sum of one block.
+// The block of B ids a lane reads for one row of a group (B = 8, the block
+// size of every run that is not flat), and its ids.
 template <int B> struct IdBlock;
-template <> struct IdBlock<2> {
-  unsigned w;
-  __device__ __forceinline__ void load(const uint16_t *p, uint64_t pol) {
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
-        : "=r"(w) : "l"(p), "l"(pol));
-  }
-  __device__ __forceinline__ unsigned id(int k) const { return k ? (w >> 16) : (w & 0xffffu); }
-};
-template <> struct IdBlock<4> {
-  unsigned w0, w1;
-  __device__ __forceinline__ void load(const uint16_t *p, uint64_t pol) {
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
-        : "=r"(w0), "=r"(w1) : "l"(p), "l"(pol));
-  }
-  __device__ __forceinline__ unsigned id(int k) const {
-    const unsigned w = k < 2 ? w0 : w1;
-    return (k & 1) ? (w >> 16) : (w & 0xffffu);
-  }
-};
 template <> struct IdBlock<8> {
   uint4 q;
   __device__ __forceinline__ void load(const uint16_t *p, uint64_t pol) {
@@ -101,7 +82,7 @@ template <> struct IdBlock<8> {
 // A warp's contiguous block of ng groups of one run (all of one shape: rows
 // rows of 32 lanes x B ids, 2^ll lanes per pair) is one regular array: item
 // i (row i % rows of group i / rows) of lane l sits at base + (32 i + l) B.
-// Each lane streams its column with U items (32-64 bytes) in flight,
+// Each lane streams its column with U items (64 bytes) in flight,
 // keeps B running sums (one per position in a block), and at the end of
 // each group joins them by a fixed tree, then across the pair's lanes by an
 // xor tree; the pair's first lane writes the partial to part[dest[32 g + p]].
@@ -295,11 +276,8 @@ slice_partial_kernel(const BlockedArgs a) {
       if (FLAT) {
         warp_flat_pairs(a, base, gw0, gw1 - gw0, lb, svb, ps);
       } else {
-        switch (lb) {
-          case 1: warp_run_groups<2>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
-          case 2: warp_run_groups<4>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
-          default: warp_run_groups<8>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps); break;
-        }
+        // every run that is not flat has blocks of 8 ids (the layout's classes)
+        warp_run_groups<8>(a, base, gw0, gw1 - gw0, rows, ll, svb, ps);
       }
     }
   }

@@ -59,11 +59,14 @@ int BitsFor(int64_t x) {  // bits needed for values in [0, x)
   return b;
 }
 
-// Length class of a pair: exact lengths 1..8, then whole 8-id blocks 2..8,
+// Length class of a pair: lengths 1, 2, 3-4 and 5-8 (one block of 1, 2, 4
+// or 8 ids: the flat classes 0, 1, 3, 7), then whole 8-id blocks 2..8,
 // then four classes per doubling of the block count.  All pairs of a class
-// share the block size B.
+// share the block size B; every class past the flat ones has B = 8.
 __host__ __device__ inline int PairClass(int len) {
-  if (len <= 8) return len - 1;
+  if (len <= 2) return len - 1;
+  if (len <= 4) return 3;  // one block of 4 ids (a length-3 pair pads one)
+  if (len <= 8) return 7;  // one block of 8 ids
   const int nb = (len + 7) >> 3;
   if (nb <= 8) return 6 + nb;
   int lg = 3;
@@ -202,7 +205,7 @@ __global__ void bin_size_kernel(int32_t nbins, const int32_t *__restrict__ bin_r
 }
 
 // Classes whose runs have one block of B ids per pair and one lane per pair
-// (exact lengths 1, 2, 4 and 8): their runs are flat (FlatShape below).
+// (lengths 1, 2, 3-4 and 5-8): their runs are flat (FlatShape below).
 __host__ __device__ inline bool ClassFlat(int cls) {
   return cls == 0 || cls == 1 || cls == 3 || cls == 7;
 }
