@@ -419,18 +419,18 @@ __global__ void iota_kernel(int64_t count, int32_t *out) {
   if (i < count) out[i] = static_cast<int32_t>(i);
 }
 
-// Entry j (pair k, its e-th id) lands in block e / B of its pair: row
-// (e / B) / L of its group, lane p L + (e / B) % L, position e % B.  In a
-// flat run (one block per pair), pair P of the run sits in block P / (32 Q)
-// of 256 ids (Q = 8 / B pairs per 16-byte chunk), chunk P % 32 of it, place
-// (P / 32) % Q in the chunk: lane c of a warp reading chunk c of a block
+// Entry j (pair k, its e-th id) of a pair of a flat run (one block of B ids
+// per pair): pair P of the run sits in block P / (32 Q) of 256 ids
+// (Q = 8 / B pairs per 16-byte chunk), chunk P % 32 of it, place (P / 32) % Q
+// in the chunk, position e: lane c of a warp reading chunk c of a block
 // holds pairs c, c + 32, ..., so the warp's stores of the pairs' partials
-// and loads of their dests are lane-consecutive.
+// and loads of their dests are lane-consecutive.  Entries of the other
+// runs are placed by place_run_ids_kernel.
 __global__ void scatter_ids_kernel(int64_t m, const int32_t *__restrict__ incl,
                                    const int32_t *__restrict__ pair_pos,
                                    const int32_t *__restrict__ slot_of,
                                    const int32_t *__restrict__ group_run,
-                                   const int4 *__restrict__ run, const int64_t *__restrict__ run_gsize,
+                                   const int4 *__restrict__ run,
                                    const uint16_t *__restrict__ lid, uint16_t *src) {
   const int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (j >= m) return;
@@ -438,23 +438,63 @@ __global__ void scatter_ids_kernel(int64_t m, const int32_t *__restrict__ incl,
   const int32_t e = static_cast<int32_t>(j - pair_pos[k]);
   const int32_t slot = slot_of[k];
   const int32_t grp = slot >> 5;
+  const int4 rd = run[group_run[grp]];
+  if (!FlatShape(rd.w)) return;
+  const int lb = rd.w & 15;
+  const int64_t P = static_cast<int64_t>(grp - rd.x) * 32 + (slot & 31);
+  const int64_t in_blk = P % (256 >> lb);
+  const int64_t pos = static_cast<int64_t>(rd.z) + (P / (256 >> lb)) * 256 +
+                      (in_blk & 31) * 8 + ((in_blk >> 5) << lb) + e;
+  src[pos] = lid[j];
+}
+
+// The ids of a pair of a run that is not flat (blocks of 8 ids, L lanes,
+// rows rows: S = 8 rows load rounds; round s = 8 row + k is the k-th id of
+// every lane's block of that row, one shared-memory load of the warp).  The
+// pair's ids are ordered by bank (id mod 32), rotated by the pair's first
+// lane p L so that pairs of a group start on different banks, and the q-th
+// id goes to round q mod S, lane p L + q / S: within a round the pair's ids
+// then fall on different banks wherever its banks hold at most S ids each
+// (ids in source order put ~3.5 lanes on one bank per load; this
+// placement about 1.6-2.2 for the long pairs of 16 and 32 lanes).  One
+// thread per pair (at most kMaxPairIds ids), a counting sort by bank.
+__global__ void place_run_ids_kernel(int64_t npairs, const int32_t *__restrict__ pair_pos,
+                                     const int32_t *__restrict__ pair_len,
+                                     const int32_t *__restrict__ slot_of,
+                                     const int32_t *__restrict__ group_run,
+                                     const int4 *__restrict__ run,
+                                     const int64_t *__restrict__ run_gsize,
+                                     const uint16_t *__restrict__ lid, uint16_t *src) {
+  const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= npairs) return;
+  const int32_t slot = slot_of[k];
+  const int32_t grp = slot >> 5;
   const int32_t r = group_run[grp];
   const int4 rd = run[r];
-  const int lb = rd.w & 15, ll = (rd.w >> 4) & 15;
-  const int32_t blk = e >> lb;
-  const int lane = ((slot & 31) << ll) + (blk & ((1 << ll) - 1));
-  const int64_t row = blk >> ll;
-  int64_t pos;
-  if (FlatShape(rd.w)) {
-    const int64_t P = static_cast<int64_t>(grp - rd.x) * 32 + (slot & 31);
-    const int64_t in_blk = P % (256 >> lb);
-    pos = static_cast<int64_t>(rd.z) + (P / (256 >> lb)) * 256 + (in_blk & 31) * 8 +
-          ((in_blk >> 5) << lb) + e;
-  } else {
-    pos = static_cast<int64_t>(rd.z) + static_cast<int64_t>(grp - rd.x) * run_gsize[r] +
-          ((row * 32 + lane) << lb) + (e & ((1 << lb) - 1));
+  if (FlatShape(rd.w)) return;  // placed by scatter_ids_kernel
+  const int ll = (rd.w >> 4) & 15, rows = rd.w >> 8;
+  const int p = slot & 31;                 // pair within the group
+  const int first_lane = p << ll;
+  const int S = rows * 8;
+  const int32_t j0 = pair_pos[k], len = pair_len[k];
+  int start[32];
+#pragma unroll
+  for (int b = 0; b < 32; b++) start[b] = 0;
+  for (int32_t e = 0; e < len; e++) start[(lid[j0 + e] - first_lane) & 31]++;
+  int acc = 0;
+#pragma unroll
+  for (int b = 0; b < 32; b++) {
+    const int c = start[b];
+    start[b] = acc;
+    acc += c;
   }
-  src[pos] = lid[j];
+  const int64_t gbase = static_cast<int64_t>(rd.z) + static_cast<int64_t>(grp - rd.x) * run_gsize[r];
+  for (int32_t e = 0; e < len; e++) {
+    const uint16_t v = lid[j0 + e];
+    const int q = start[(v - first_lane) & 31]++;
+    const int round = q % S, lane = first_lane + q / S;
+    src[gbase + ((static_cast<int64_t>(round >> 3) * 32 + lane) << 3) + (round & 7)] = v;
+  }
 }
 
 // Phase-2 stream element j2 = pair k2[j2] of row u2[j2]: its position in
@@ -822,7 +862,10 @@ cudaError_t BuildSliceBlocks(const DeviceGraph &g, int slice_verts, int bin_word
   fill_u16_kernel<<<Blocks(elems + 64, T), T, 0, s>>>(elems + 64,
                                                       static_cast<uint16_t>(slice_verts), sb->src);
   scatter_ids_kernel<<<Blocks(m, T), T, 0, s>>>(m, incl, pair_pos, slot_of, group_run, sb->run,
-                                                run_gsize, lid, sb->src);
+                                                lid, sb->src);
+  place_run_ids_kernel<<<Blocks(npairs, T), T, 0, s>>>(npairs, pair_pos, pair_len, slot_of,
+                                                       group_run, sb->run, run_gsize, lid,
+                                                       sb->src);
   SB_TRY(Keep(sb, &sb->part, part_len));
   SB_TRY(cudaMemsetAsync(sb->part, 0, sizeof(float) * part_len, s));
   SB_TRY(cudaGetLastError());
