@@ -3,8 +3,8 @@
 For each graph: sweeps (GPU / reference FP32 restatement), L1 and max-abs
 error of the GPU scores against the FP64 oracle, the same for the
 reference's FP32 scores (the oracle's bit-exact restatement of
-src/pr_spmv.cc:35-61), the PRVerifier total error of the GPU scores, and the
-sweep layout the engine used (slice-blocked or gather, its default choice).
+src/pr_spmv.cc:35-61), and the PRVerifier total error of the GPU scores,
+once per sweep layout (slice-blocked and gather, each forced).
 Prints a markdown table.  Needs a GPU; run as `python tests/parity_report.py`.
 """
 import os
@@ -28,8 +28,9 @@ def main():
     print("| graph | N | M | sweeps GPU / ref | L1(GPU-fp64) | max abs(GPU-fp64) "
           "| L1(ref fp32-fp64) | max abs(ref-fp64) | PRVerifier error (GPU) | sweep |")
     print("|---|---:|---:|---|---:|---:|---:|---:|---:|---|")
-    for args in GRAPHS:
+    for args, layout in [(a, l) for a in GRAPHS for l in ("blocked", "gather")]:
         g = make_graph(args)
+        eng.set_sweep_layout(layout)
         eng.upload(g)
         res = eng.run(20, 1e-4)
         s = res.scores.astype(np.float64)
