@@ -5,7 +5,7 @@
 // that misses L1 costs one 32-byte sector request between the SM and L2, and
 // those requests, not HBM bytes, bound the classic sweep (pull.cu).  This
 // layout replaces them with streamed bytes (propagation blocking, Beamer,
-// Asanovic and Patterson, IPDPS 2017), in two kernels per sweep:
+// Asanovic and Patterson, IPDPS 2017), in two phases per sweep:
 //
 //   phase 1 (per source slice)  a CTA holds contrib[] of one slice of
 //     slice_verts consecutive (renumbered) source ids in shared memory.  The
@@ -13,18 +13,21 @@
 //     stored sliced-ELL: grouped by length class into groups of 32 lanes,
 //     L lanes per pair (1 to 32, chosen per run of a class), the
 //     16-bit slice-local source ids of each lane's share interleaved across
-//     the group in blocks of B ids (B = 1, 2, 4 or 8 by length, padded with
-//     an id whose value is zero).  All groups of one (slice, class) run
-//     have the same shape, so a warp streams a contiguous block of groups as
-//     one regular array.  The pair's lanes join their sums and write the
-//     partial to part[dest[pair]].
+//     the group in blocks of B ids (pairs of up to 8 ids: one block of 1, 2,
+//     4 or 8; longer pairs: blocks of 8; padded with an id whose value is
+//     zero).  All groups of one (slice, class) run have the same shape, so a
+//     warp streams a contiguous block of groups as one regular array.  The
+//     pair's lanes join their sums and write the partial to
+//     part[dest[pair]].  Two launches: the runs of one block per pair (flat)
+//     and the others.
 //   phase 2 (per destination bin)  part[] is laid out bin-major: the
-//     partials of one bin of consecutive rows are one contiguous block
-//     (slice-major inside).  A CTA copies that block into shared memory;
-//     each thread then takes rows of the bin and sums each row's partials
-//     in slice order (a 16-bit position in the block per pair, rows' pairs
-//     consecutive), and updates the row: new = base + d * sum, |new - old|
-//     added in FP64, contrib[u] = new / out_degree(u).
+//     partials of one bin of consecutive rows are one contiguous block (the
+//     flat launch's pairs first, each part slice-major).  A CTA copies that
+//     block and the bin's positions into shared memory; each thread then
+//     takes rows of the bin and sums each row's partials in slice order (a
+//     16-bit position in the block per pair, rows' pairs consecutive), and
+//     updates the row: new = base + d * sum, |new - old| added in FP64,
+//     contrib[u] = new / out_degree(u).
 //
 // Every sum is a fixed tree over a fixed layout, so a sweep's result does
 // not depend on scheduling.  With vertices in descending-degree order most
