@@ -6,8 +6,8 @@ include/pr_gpu.h; graphs come from the host builder ``lib/libgapbs_graph.so``
 """
 from .graph import Builder, Graph, GraphBuildError, generate, make_graph
 from .pagerank import (K_DAMP, PageRankEngine, PageRankError, PageRankPull, PageRankResult,
-                       PersonalizedPageRank, engine_for, top_scores)
+                       PersonalizedPageRank, PRVerifier, engine_for, top_scores)
 
 __all__ = ["Builder", "Graph", "GraphBuildError", "generate", "make_graph", "K_DAMP",
            "PageRankEngine", "PageRankError", "PageRankPull", "PageRankResult",
-           "PersonalizedPageRank", "engine_for", "top_scores"]
+           "PersonalizedPageRank", "PRVerifier", "engine_for", "top_scores"]

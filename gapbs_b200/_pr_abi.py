@@ -27,7 +27,8 @@ SYMBOLS = (
     "pr_gpu_set_batch_tile", "pr_gpu_get_batch_tile", "pr_gpu_set_sweep_layout",
     "pr_gpu_sweep_layout_info", "pr_gpu_sweep_kernel_times", "pr_gpu_last_timing",
     "pr_gpu_set_edge_weights_device", "pr_gpu_set_batch_schedule", "pr_gpu_get_batch_schedule",
-    "pr_gpu_graph_info", "pr_gpu_measure_gather_rate", "pr_gpu_measure_row_gather_rate", "pr_gpu_run_noalloc", "pr_gpu_destroy", "pr_gpu_last_error",
+    "pr_gpu_verify", "pr_gpu_graph_info", "pr_gpu_measure_gather_rate",
+    "pr_gpu_measure_row_gather_rate", "pr_gpu_run_noalloc", "pr_gpu_destroy", "pr_gpu_last_error",
 )
 
 
@@ -71,6 +72,8 @@ def declare(lib):
     lib.pr_gpu_sweep_kernel_times.argtypes = [P, c_int, c_double, POINTER(c_double), c_int,
                                               POINTER(c_int), POINTER(c_int32)]
     lib.pr_gpu_sweep_kernel_times.restype = c_int
+    lib.pr_gpu_verify.argtypes = [P, P, c_float, POINTER(c_double)]
+    lib.pr_gpu_verify.restype = c_int
     lib.pr_gpu_set_batch_schedule.argtypes = [P, c_int, c_int]
     lib.pr_gpu_set_batch_schedule.restype = c_int
     lib.pr_gpu_get_batch_schedule.argtypes = [P, POINTER(c_int), POINTER(c_int), POINTER(c_int)]

@@ -167,6 +167,14 @@ void FreeDeviceGraph(DeviceGraph *g);
 cudaError_t UpdateDeviceWeights(DeviceGraph *g, const float *d_w, cudaStream_t s,
                                 std::string *err);
 
+// The reference's PRVerifier residuals (verify.cu): score_orig holds n
+// scores in original ids; contrib (n floats, scratch) receives score /
+// out_degree in new ids and resid_orig[v] = |base + d * incoming[v] -
+// score[v]| in original ids, incoming summed in row order.  Edge weights are
+// not used.
+cudaError_t VerifyResiduals(const DeviceGraph &g, const float *score_orig, float damping,
+                            float *contrib, float *resid_orig, cudaStream_t s);
+
 // The reference's -g / -u graph built on the device (generate.cu): CSR of
 // the symmetrised, squished graph in original ids, int32 offsets (n+1) and
 // neighbours (m), owned by the caller.  perm_host: the R-MAT relabelling.

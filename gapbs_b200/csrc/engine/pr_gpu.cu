@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -1072,6 +1073,29 @@ int pr_gpu_adjoint(pr_gpu_t *h, int max_iters, double epsilon, float damping,
   if (grad_teleport) rc = CopyToHost(h, grad_teleport, sc.outbuf, sizeof(float) * n);
   if (!rc && grad_edge_w) rc = CopyToHost(h, grad_edge_w, sc.edge_buf, sizeof(float) * m);
   return rc;
+}
+
+int pr_gpu_verify(pr_gpu_t *h, const float *scores, float damping, double *error_out) {
+  if (!h) return PR_GPU_EINVAL;
+  if (!h->has_graph) return SetErr(h, PR_GPU_ENOGRAPH, "no graph uploaded");
+  if (!scores || !error_out) return SetErr(h, PR_GPU_EINVAL, "scores or error_out is null");
+  PR_CHECK(h, cudaSetDevice(h->device));
+  const int64_t n = h->g.n;
+  int rc = EnsureScratch(h, n, 1, 1, 1);
+  if (!rc) rc = CopyToDevice(h, h->sc.tele, scores, sizeof(float) * n);
+  if (rc) return rc;
+  PR_CHECK(h, prgpu::VerifyResiduals(h->g, h->sc.tele, damping, h->sc.contrib[0], h->sc.outbuf,
+                                     h->stream));
+  std::unique_ptr<float[]> resid(new (std::nothrow) float[n]);
+  if (!resid) return SetErr(h, PR_GPU_ENOMEM, "host buffer for the residuals");
+  rc = CopyToHost(h, resid.get(), h->sc.outbuf, sizeof(float) * n);
+  if (rc) return rc;
+  // the reference's L1 sum: each float residual added in double, in vertex
+  // order (src/pr_spmv.cc:88-91)
+  double error = 0;
+  for (int64_t v = 0; v < n; v++) error += static_cast<double>(resid[v]);
+  *error_out = error;
+  return PR_GPU_OK;
 }
 
 int pr_gpu_set_batch_tile(pr_gpu_t *h, int width) {

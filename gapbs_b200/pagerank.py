@@ -317,6 +317,19 @@ class PageRankEngine:
                 "pairs": pairs.value, "ids": ids.value, "bytes": nbytes.value,
                 "last_run_blocked": bool(last.value)}
 
+    def verify(self, scores, damping: float = float(K_DAMP)) -> float:
+        """The reference's PRVerifier error (src/pr_spmv.cc:78-94) of `scores`
+        (n float32 in original ids) on the uploaded graph, computed on the
+        device (pr_gpu_verify): bit-identical to the reference's when every
+        in-row lists its sources in ascending order, as the builder's do."""
+        s = np.ascontiguousarray(scores, dtype=np.float32)
+        if s.ndim != 1 or s.shape[0] != self.n:
+            raise ValueError("scores must hold one float per vertex")
+        err = c_double()
+        self._check(self._lib.pr_gpu_verify(self._h, _ptr(s), float(damping), byref(err)),
+                    "pr_gpu_verify")
+        return err.value
+
     def sweep_kernel_times(self, max_iters: int = 20, epsilon: float = 1e-4):
         """One plain solve with every sweep kernel timed on its own
         (pr_gpu_sweep_kernel_times): the average device ms per sweep of each
@@ -398,6 +411,15 @@ def PageRankPull(g: Graph, max_iters: int, epsilon: float = 0.0,
         for i in range(res.num_sweeps):
             print_step(i, float(res.err_trace[i, 0]))
     return res.scores
+
+
+def PRVerifier(g: Graph, scores, target_error: float, device: int = 0) -> bool:
+    """Drop-in for src/pr_spmv.cc:78-94: prints the reference's "Total Error"
+    line (src/util.h PrintTime format) and returns error < target_error; the
+    error is computed on the device (PageRankEngine.verify)."""
+    error = engine_for(g, device).verify(scores, float(K_DAMP))
+    print(f"{'Total Error:':<21}{error:3.5f}")
+    return error < target_error
 
 
 def PersonalizedPageRank(g: Graph, teleport, max_iters: int = 20, epsilon: float = 1e-4,

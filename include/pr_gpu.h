@@ -195,6 +195,21 @@ int pr_gpu_adjoint_device(pr_gpu_t *h, int max_iters, double epsilon,
                           const float *scores_dev, float *grad_teleport_dev,
                           float *grad_edge_w_dev, int32_t *sweeps_out);
 
+/* The reference's PRVerifier (src/pr_spmv.cc:78-94) on the device: one
+ * push-direction sweep from `scores` (n floats in original ids, host buffer),
+ *   error = sum_n |base + d * incoming[n] - scores[n]|,
+ *   incoming[n] = sum over in-neighbours u of scores[u] / out_degree(u),
+ * base = (1 - d) / N, every per-vertex operation in float as the reference
+ * computes it and the sum over vertices in double in vertex order.  When each
+ * row of the uploaded in-CSR lists its sources in ascending order (the
+ * reference's builder sorts and deduplicates every row), incoming[n] is added
+ * in the reference's push order and *error_out equals the reference's error
+ * bit for bit; other row orders change only its rounding.  Edge weights, if
+ * uploaded, are not used: this is the unweighted check.  The caller compares
+ * *error_out with its tolerance (the reference passes when error < target).
+ * damping is the reference's kDamp (0.85f). */
+int pr_gpu_verify(pr_gpu_t *h, const float *scores, float damping, double *error_out);
+
 /* Engine controls below have no counterpart in the reference.
  *
  * Column tile width of batched (ncols > 1) solves: 8, 16, 32 or 64 score

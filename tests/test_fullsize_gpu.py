@@ -88,8 +88,10 @@ def test_pagerankpull_fullsize(engine, case, layout):
     order = np.lexsort((np.arange(s.size), -s.astype(np.float64)))[:5]
     assert [int(i) for i in order] == top
     assert abs(float(s.astype(np.float64).sum()) - e["scores_sum"]) <= 1e-5 * e["scores_sum"]
-    # the reference's verifier
-    assert oracle.pr_verify_f32(g, s) < 1e-4
+    # the reference's verifier; the device verifier gives its error bit for bit
+    e_or = oracle.pr_verify_f32(g, s)
+    assert e_or < 1e-4
+    assert engine.verify(s) == e_or
 
 
 @pytest.mark.parametrize("case", ["u24", "g25"])
