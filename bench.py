@@ -17,6 +17,9 @@ scores written in the caller's vertex order).  Prints ONE JSON line on rank 0:
                on this host's cores, bounded sample
   ppr          batched personalized PageRank (64 teleport vectors, Kronecker
                scale 22) vs 64 sequential single-vector solves
+  verify       the reference's PRVerifier on the device (pr_gpu_verify) on
+               the timed solve's scores, beside the reference's serial one
+               on the same scores (whose error must be the same double)
 
 --gpus N under torchrun: N independent replicas (the path does not shard),
 timed as the max over ranks.  --impl reference: the reference arm (rank 0).
@@ -62,6 +65,7 @@ def parse_args():
     p.add_argument("--bfs-sources", type=int, default=8)
     p.add_argument("--e2e-upload-steps", type=int, default=5,
                    help="steps of the end-to-end variant that uploads the graph every step")
+    p.add_argument("--no-verify", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-trials", type=int, default=2)
     return p.parse_args()
@@ -344,6 +348,23 @@ def run_ours(a, dist: Dist):
     e2e_edges = dist.sum(float(m) * e2e_sweeps)
     e2e_value = e2e_edges / e2e_s / 1e9
 
+    # ---- the reference's PRVerifier on the device (pr_gpu_verify: the host
+    # scores of the last solve in, the error out) on the same graph
+    verify = None
+    if not a.no_verify:
+        scores_v = np.array(host_out, copy=True)
+        eng.verify(scores_v)  # warm-up
+        vt = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            err_v = eng.verify(scores_v)
+            vt.append(time.perf_counter() - t0)
+        verify = {"workload": f"PRVerifier of the timed solve's scores on {a.graph.strip()}",
+                  "ms": round(dist.max(float(np.median(vt))) * 1e3, 3),
+                  "unit": "ms per call (C ABI: host scores in, error out; copies included)",
+                  "statistic": "median of 3 calls", "error": err_v,
+                  "passes": bool(err_v < a.epsilon)}
+
     # ---- connected components (the reference's Afforest) on the same graph
     cc = None
     if not a.no_cc:
@@ -539,6 +560,8 @@ def run_ours(a, dist: Dist):
         }
     if e2e_up is not None:
         result["e2e_graph_upload_each_step"] = e2e_up
+    if verify is not None:
+        result["verify"] = verify
     if cc is not None:
         result["cc"] = cc
     if bfs is not None:
@@ -555,7 +578,22 @@ def run_ours(a, dist: Dist):
     if not a.no_cpu_baseline and dist.rank == 0 and dist.world == 1:
         if g is None:
             g = eng.download_graph()  # the generated graph, for the reference on the host
-        result["cpu_baseline"] = cpu_baseline(g, a, sweeps_per_step, max_ms / a.steps)
+        import oracle
+        rg = oracle.RefGraph.from_csr(g) if oracle.ref_available() else None
+        result["cpu_baseline"] = cpu_baseline(g, a, sweeps_per_step, max_ms / a.steps, rg)
+        if verify is not None and rg is not None:
+            # the reference's serial PRVerifier on the same scores, at the
+            # device's error e and at the next double above it: false then
+            # true only when the reference's error is exactly e
+            e_v = verify["error"]
+            t0 = time.perf_counter()
+            below_e, _ = capture_fd1(rg.verify, scores_v, e_v)
+            below_next, _ = capture_fd1(rg.verify, scores_v, float(np.nextafter(e_v, np.inf)))
+            sec = (time.perf_counter() - t0) / 2
+            verify["reference_cpu_ms"] = round(sec * 1e3, 1)
+            verify["reference_cpu_cores"] = 1
+            verify["reference_error_equal"] = bool(not below_e and below_next)
+            verify["speedup_vs_reference_cpu"] = round(sec * 1e3 / verify["ms"], 1)
         if bfs is not None and bfs["sources"]:
             import oracle
             if oracle.ref_available():
@@ -757,12 +795,11 @@ def run_adjoint(a, dev):
     }
 
 
-def cpu_baseline(g, a, gpu_sweeps, gpu_ms_per_solve):
+def cpu_baseline(g, a, gpu_sweeps, gpu_ms_per_solve, rg=None):
     import oracle
     cores = os.cpu_count() or 1
     n, m = g.num_nodes, g.num_edges_directed
-    if oracle.ref_available():
-        rg = oracle.RefGraph.from_csr(g)
+    if rg is not None:
         tot, per = rg.time_pagerank_pull(trials=a.cpu_trials, max_iters=a.max_iters,
                                          epsilon=a.epsilon)
         sweeps = gpu_sweeps
