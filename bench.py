@@ -17,6 +17,8 @@ scores written in the caller's vertex order).  Prints ONE JSON line on rank 0:
                on this host's cores, bounded sample
   ppr          batched personalized PageRank (64 teleport vectors, Kronecker
                scale 22) vs 64 sequential single-vector solves
+  noalloc      pr_gpu_run_noalloc (no device allocation) at its size limit,
+               beside the regular entry point on the same graph
   verify       the reference's PRVerifier on the device (pr_gpu_verify) on
                the timed solve's scores, beside the reference's serial one
                on the same scores (whose error must be the same double)
@@ -66,6 +68,9 @@ def parse_args():
     p.add_argument("--e2e-upload-steps", type=int, default=5,
                    help="steps of the end-to-end variant that uploads the graph every step")
     p.add_argument("--no-verify", action="store_true")
+    p.add_argument("--noalloc-graph", default="-g 20",
+                   help="graph of the no-allocation entry point's leg (at most 2^20 vertices)")
+    p.add_argument("--no-noalloc", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-trials", type=int, default=2)
     return p.parse_args()
@@ -573,6 +578,11 @@ def run_ours(a, dist: Dist):
         result["ppr"] = run_ppr(a, dev)
     if not a.no_adjoint and dist.rank == 0:
         result["adjoint"] = run_adjoint(a, dev)
+    if not a.no_noalloc and dist.rank == 0:
+        try:
+            result["noalloc"] = run_noalloc(a, dev)
+        except Exception as exc:  # a side leg: its failure must not lose the bench line
+            result["noalloc"] = {"error": f"{type(exc).__name__}: {exc}"}
 
     # ---- CPU baseline on this host (rank 0 at N=1 only)
     if not a.no_cpu_baseline and dist.rank == 0 and dist.world == 1:
@@ -710,6 +720,66 @@ def run_ppr(a, dev):
         "speedup_aggregate_gteps": round(b_gteps / s_gteps, 3),
         "max_l1_batched_vs_single": maxdiff,
     }
+
+
+def run_noalloc(a, dev):
+    """pr_gpu_run_noalloc (the entry point that allocates nothing; its sweep
+    has no degree bins) on the largest graph it takes, beside the regular
+    entry point (pr_gpu_run_device) on the same graph: device buffers in and
+    out, CUDA events on the stream both run on, inputs resident."""
+    import ctypes
+    import torch
+    from gapbs_b200 import PageRankEngine
+    from gapbs_b200._native import pr_lib
+    eng = PageRankEngine(dev)
+    n, m = eng.generate(a.noalloc_graph)
+    g = eng.download_graph()
+    stream = torch.cuda.current_stream(dev)
+    eng.set_stream(stream.cuda_stream)
+    d = f"cuda:{dev}"
+    out = torch.empty(n, dtype=torch.float32, device=d)
+    out_na = torch.empty(n, dtype=torch.float32, device=d)
+    in_off = torch.tensor(np.asarray(g.in_offsets, np.int32), device=d)
+    in_nbr = torch.tensor(np.asarray(g.in_neighbors, np.int32), device=d)
+    reps = max(3, a.steps)
+    sweeps = np.zeros(1, np.int32)
+    msg = ctypes.create_string_buffer(256)
+
+    def noalloc():
+        rc = pr_lib().pr_gpu_run_noalloc(dev, n, m, in_off.data_ptr(), in_nbr.data_ptr(), None,
+                                         a.max_iters, a.epsilon, 0.85, out_na.data_ptr(),
+                                         sweeps.ctypes.data, None, stream.cuda_stream, msg, 256)
+        if rc != 0:
+            raise RuntimeError(f"pr_gpu_run_noalloc: {rc} {msg.value.decode()}")
+        return int(sweeps[0])
+
+    def regular():
+        sw, _ = eng.run_device(a.max_iters, a.epsilon, 0.85, 1, None, out.data_ptr())
+        return int(sw[0])
+
+    timed = {}
+    for name, fn in (("regular", regular), ("noalloc", noalloc)):
+        for _ in range(max(1, a.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        total = sum(fn() for _ in range(reps))
+        e.record(stream)
+        torch.cuda.synchronize()
+        ms = s.elapsed_time(e) / reps
+        timed[name] = (ms, total / reps)
+    ref = out.cpu().numpy().astype(np.float64)
+    got = out_na.cpu().numpy().astype(np.float64)
+    eng.close()
+    (r_ms, r_sw), (n_ms, n_sw) = timed["regular"], timed["noalloc"]
+    return {"workload": f"PageRankPull {a.noalloc_graph.strip()} (N={n}, M={m}) through "
+                        "pr_gpu_run_noalloc, beside pr_gpu_run_device",
+            "noalloc_ms": round(n_ms, 3), "noalloc_gteps": round(m * n_sw / n_ms / 1e6, 2),
+            "regular_ms": round(r_ms, 3), "regular_gteps": round(m * r_sw / r_ms / 1e6, 2),
+            "sweeps": n_sw, "regular_sweeps": r_sw,
+            "max_rel_diff": float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-30))),
+            "statistic": f"mean of {reps} solves (CUDA events, device buffers)"}
 
 
 def run_adjoint(a, dev):
