@@ -47,3 +47,22 @@ def test_row_order_equals_push_order(golden, case):
     for s in (rng.random(n, dtype=np.float32) / np.float32(n),
               np.asarray(converged, np.float32)):
         assert row_order_error(g, s) == oracle.pr_verify_f32(g, s)
+
+
+def test_reversed_rows_change_the_error():
+    """The check has teeth: with every in-row reversed (descending source
+    order) the same computation no longer gives the push-order error."""
+    g = make_graph("-g 10")
+
+    class Reversed:
+        pass
+    r = Reversed()
+    r.num_nodes, r.out_offsets = g.num_nodes, g.out_offsets
+    r.in_offsets = np.asarray(g.in_offsets, np.int64)
+    nbr = np.asarray(g.in_neighbors, np.int64).copy()
+    for v in range(g.num_nodes):
+        nbr[r.in_offsets[v]:r.in_offsets[v + 1]] = nbr[r.in_offsets[v]:r.in_offsets[v + 1]][::-1]
+    r.in_neighbors = nbr
+    s = np.random.default_rng(21).random(g.num_nodes, dtype=np.float32) / np.float32(g.num_nodes)
+    assert row_order_error(g, s) == oracle.pr_verify_f32(g, s)
+    assert row_order_error(r, s) != oracle.pr_verify_f32(g, s)
