@@ -59,9 +59,10 @@ __device__ __forceinline__ void write_residual(int64_t u, float sum,
 // One warp per row of [0, nrows) (grid-stride over rows): the row's contribs
 // are fetched 32 at a time, the next 32 while the current ones are added;
 // every lane keeps the same running sum.  A full chunk's 32 broadcasts are
-// unrolled, so they are issued ahead of their adds and only the adds' own
-// latency stays on the chain (the largest rows, a million entries at
-// Kronecker scale 25, are one warp's sequential sum each).
+// unrolled, so they are issued ahead of their adds.  The longest rows bound
+// the kernel: each is one warp's sequential sum, fetched one chunk ahead, so
+// the longest row at Kronecker scale 25 (639,467 entries) waits on memory
+// about 20,000 times in turn.
 __global__ void __launch_bounds__(kVerifyThreads, 4)
 verify_long_rows_kernel(int64_t nrows, const int32_t *__restrict__ rowoff,
                         const int32_t *__restrict__ col, const float *__restrict__ contrib,
